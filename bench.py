@@ -1,0 +1,430 @@
+#!/usr/bin/env python
+"""DM-trial x Msamples/s of batched MS-OSM coherent dedispersion + folding.
+
+Workload (one step): 16 MHz complex baseband centred at 1250 MHz (lower edge
+1242 MHz), 2^26 complex64 samples carrying an injected pulsar (DM 73.2,
+P = 3.1 ms, Gaussian pulse of 3% duty cycle, peak per-sample SNR 0.05, seeded
+synthetic data), dedispersed at 256 DM trials uniform over 0-100 pc/cm^3 with
+FFT 4096 (MS-OSM, per-bin block delays), |y|^2 detection and folding into
+1024 phase bins per trial, all through libmsosm_b200.so.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference|reference-gpu]
+
+`value`: device time (CUDA events) with the input resident in HBM.  `e2e`:
+the same metric through the C ABI with pinned HOST input, the host->device
+copy of every step and the device->host read of the folded profiles inside
+the timed region.  `--impl reference` times the oracle (the FP64 C
+restatement of the reference algorithm, OpenMP over trials) on the host
+cores on a bounded sample; `--impl reference-gpu` times the reference's own
+cuFFT classes built for sm_100a (oracle/_ref/ref_gpu_runner) when present.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+BW = 16e6
+F0 = 1242e6  # lower band edge: centre 1250 MHz
+LOG2_SAMPLES = 26
+N_DM = 256
+DM_MAX = 100.0
+FFTPOINT = 4096
+NBINS = 1024
+PULSAR = dict(dm=73.2, period=3.1e-3, fwhm=0.03, snr=0.05, seed=0)
+METRIC = "DM-trial x Msamples/s (MS-OSM dedispersion + |y|^2 fold, FFT 4096, 256 trials), 1 B200"
+UNIT = "DM-trial*Msamples/s"
+
+
+def log(*a):
+    print(*a, file=sys.stderr, flush=True)
+
+
+def dist_setup():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def workload_config(samples, n_dm, ws):
+    return {"workload": "batched multi-DM MS-OSM: 16 MHz @ 1250 MHz, 2^%d complex64 samples, %d DM trials "
+                        "0-100 per GPU, FFT %d, fold %d bins" % (int(math.log2(samples)), n_dm, FFTPOINT, NBINS),
+            "samples_per_step": samples, "dm_trials_per_gpu": n_dm, "dm_range_per_gpu": [0.0, DM_MAX],
+            "fftpoint": FFTPOINT, "fold_bins": NBINS, "detect": "|y|^2", "period_s": PULSAR["period"],
+            "injected_dm": PULSAR["dm"], "parallelism": f"dm-shard x{ws}",
+            "l2": "inputs larger than L2 (537 MB input, 1.1 GB spectrum ring)"}
+
+
+def dm_trials(rank, n_dm):
+    # weak scaling: rank r owns trials [r*100, (r+1)*100]
+    return (np.linspace(0.0, DM_MAX, n_dm) + rank * DM_MAX).astype(np.float32)
+
+
+def make_signal(samples):
+    from msosm_gpu_b200 import simulate as S
+    t = time.time()
+    x = S.pulsar_baseband(samples, BW, F0, PULSAR["dm"], PULSAR["period"], PULSAR["fwhm"], PULSAR["snr"],
+                          seed=PULSAR["seed"])
+    log(f"signal: {samples} samples generated in {time.time() - t:.1f} s")
+    return x
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, uuid: str | None):
+        self.proc = None
+        self.uuid = uuid
+
+    def __enter__(self):
+        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200"]
+        if self.uuid:
+            cmd += ["-i", self.uuid]
+        try:
+            self.proc = subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [l for l in out.splitlines() if l.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], 0.0, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in getattr(self, "lines", []):
+            f = [v.strip() for v in l.split(",")]
+            try:
+                sm.append(float(f[0]))
+                mx = max(mx, float(f[1]))
+            except (ValueError, IndexError):
+                continue
+            for n, v in zip(names, f[4:8]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"], "samples": 0}
+        loaded = [v for v in sm if v > 0.3 * mx] or sm
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the oracle on the host cores
+# ---------------------------------------------------------------------------
+
+def cpu_baseline(dms, x, budget_s=12.0):
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    threads = os.cpu_count() or 1
+    O.lib().orc_set_threads(threads)
+    count = 8
+    d = O.Dedisp(BW, dms, F0, FFTPOINT, count, threads=threads)
+    blk = count * d.M
+    folds = [O.Fold(PULSAR["period"], BW, blk, NBINS) for _ in dms]
+    nd = int(max(d.Nd))
+    for f in folds:
+        f.discard_samples(nd)
+
+    def one(c):
+        seg = x[(c * blk) % (x.size - blk):][:blk].astype(np.complex128)
+        y = d.filter(seg)
+        for i, f in enumerate(folds):
+            f.fold_data(np.abs(y[i]) ** 2)
+
+    t = time.perf_counter()
+    one(0)
+    first = time.perf_counter() - t
+    calls = max(1, min(64, int(budget_s / max(first, 1e-3))))
+    t = time.perf_counter()
+    for c in range(1, calls + 1):
+        one(c)
+    el = time.perf_counter() - t
+    v = len(dms) * calls * blk / el / 1e6
+    return {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{len(dms)} trials x {calls * blk} samples ({calls} calls of {blk}), FP64 oracle "
+                      f"(oracle/orc.c, radix-2 FFT, OpenMP over trials) incl. |y|^2 fold, {el:.1f} s"}
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+
+def fp32_peak_tflops(torch):
+    torch.backends.cuda.matmul.allow_tf32 = False
+    n = 8192
+    a = torch.randn(n, n, device="cuda")
+    b = torch.randn(n, n, device="cuda")
+    best = 0.0
+    for i in range(6):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        torch.matmul(a, b)
+        e.record()
+        torch.cuda.synchronize()
+        if i:
+            best = max(best, 2 * n ** 3 / (s.elapsed_time(e) * 1e-3) / 1e12)
+    del a, b
+    return best
+
+
+def load_traffic():
+    p = os.path.join(ROOT, "profiles", "roofline_traffic.json")
+    if os.path.exists(p):
+        return json.load(open(p))
+    return None
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+    from msosm_gpu_b200 import Dedisperser
+
+    ws, rank, local = dist_setup()
+    if ws > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=120))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    samples = 1 << args.log2_samples
+    dms = dm_trials(rank, args.dms)
+    x = make_signal(samples)
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    fp32 = fp32_peak_tflops(torch)
+
+    # ---- value: input resident in HBM, one call per step -----------------
+    blocks = samples // (FFTPOINT // 2)
+    stream = torch.cuda.Stream(dev)
+    d = Dedisperser(BW, dms, F0, FFTPOINT, count=blocks, series=False)
+    d.set_stream(stream)
+    nd_max = int(d.Nd.max())
+    d.fold_init(PULSAR["period"], BW, time_bin=NBINS, discard_Nd=nd_max, detect="power")
+    xd = torch.from_numpy(x).to(dev)
+    torch.cuda.synchronize()
+    for _ in range(args.warmup):
+        d.filter_block(xd)
+    torch.cuda.synchronize()
+    d.enable_timing(True)
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        pass
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(uuid) as clk:
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            s.record(stream)
+            for _ in range(args.steps):
+                d.filter_block(xd)
+            e.record(stream)
+        torch.cuda.synchronize()
+    if ws > 1:
+        dist.barrier()
+    ms = s.elapsed_time(e) / args.steps
+    tm = d.timing()
+    t_ms = torch.tensor([ms], dtype=torch.float64, device=dev)
+    if ws > 1:
+        dist.all_reduce(t_ms, op=dist.ReduceOp.MAX)
+    ms_max = float(t_ms.item())
+    units = float(args.dms) * samples * ws
+    value = units / (ms_max * 1e-3) / 1e6
+    prof = d.get_profiles()
+    peak_dm = float(dms[int(np.argmax(prof.max(1) - np.median(prof, 1)))])
+
+    # ---- e2e: pinned host input through the C ABI, chunked calls -----------
+    e_count = min(blocks, 4096)
+    calls = blocks // e_count
+    de = Dedisperser(BW, dms, F0, FFTPOINT, count=e_count, series=False)
+    de.fold_init(PULSAR["period"], BW, time_bin=NBINS, discard_Nd=nd_max, detect="power")
+    xh = torch.from_numpy(x).pin_memory().numpy()
+    chunk = e_count * (FFTPOINT // 2)
+
+    def e2e_step():
+        for c in range(calls):
+            de.filter_block(xh[c * chunk:(c + 1) * chunk])
+        return de.get_profiles()
+
+    for _ in range(args.warmup):
+        e2e_step()
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        e2e_step()
+    torch.cuda.synchronize()
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    t_e = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
+    if ws > 1:
+        dist.all_reduce(t_e, op=dist.ReduceOp.MAX)
+    e2e_v = units / float(t_e.item()) / 1e6
+
+    # ---- roofline of the dominant kernel (dedisp_kernel) -------------------
+    log2n = int(math.log2(FFTPOINT))
+    flops_per_sample = 10 * log2n + 16
+    launch_samples = float(args.dms) * samples
+    dedisp_ms = tm["dedisp_ms"] / max(tm["calls"], 1)
+    achieved = flops_per_sample * launch_samples / (dedisp_ms * 1e-3) / 1e12
+    traffic = None
+    tr = load_traffic()
+    if tr and tr.get("bytes_per_dm_sample"):
+        traffic = tr["bytes_per_dm_sample"] * launch_samples
+    roofline = {"bound": "fp32", "achieved": achieved, "peak": fp32, "unit": "TFLOP/s",
+                "frac": achieved / fp32 if fp32 else None, "traffic": traffic,
+                "kernel": f"dedisp_kernel<{log2n}> (gather x H, inverse FFT, discard, |y|^2, fold)",
+                "flops_per_dm_sample": flops_per_sample,
+                "kernel_ms": dedisp_ms,
+                "peak_source": "cuBLAS SGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP32 "
+                               "figure; its bf16 tensor peak does not apply to an FP32 FFT)",
+                "stage_ms_per_step": {"forward": tm["forward_ms"] / max(tm["calls"], 1),
+                                      "dedisp": dedisp_ms,
+                                      "fold": tm["fold_ms"] / max(tm["calls"], 1)}}
+    hbm = peaks.get("hbm_gbs")
+    algo_bytes = 8.0 * samples  # the input, read once for all trials
+    roofline_hbm = {"bound": "hbm", "algorithmic_bytes_per_step": algo_bytes,
+                    "achieved_gbs": algo_bytes / (ms_max * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
+                    "note": "the fused path reads the input once for all trials; it is compute-bound"}
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded pulsar + AWGN)",
+            "config": workload_config(samples, args.dms, ws),
+            "e2e": {"value": e2e_v, "unit": UNIT, "h2d_bytes_per_step": int(x.nbytes),
+                    "d2h_bytes_per_step": int(prof.nbytes), "ms_per_step": e2e_s * 1e3,
+                    "calls_per_step": calls},
+            "gpu_launches": int(tm["kernel_launches"]),
+            "roofline": roofline, "roofline_hbm": roofline_hbm,
+            "clocks": clk.summary(),
+            "check": {"detected_dm": peak_dm, "injected_dm": PULSAR["dm"]}}
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        line["cpu_baseline"] = cpu_baseline(dms, x)
+    d.close()
+    de.close()
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# reference arms
+# ---------------------------------------------------------------------------
+
+def run_reference(args):
+    ws, rank, _ = dist_setup()
+    if rank != 0:
+        return
+    samples = 1 << args.log2_samples
+    dms = dm_trials(0, args.dms)
+    x = make_signal(min(samples, 1 << 22))
+    vals, cb = [], None
+    for _ in range(args.warmup + args.steps):
+        cb = cpu_baseline(dms, x, budget_s=max(2.0, 60.0 / max(args.steps, 1)))
+        vals.append(cb["value"])
+    vals = vals[args.warmup:] or vals
+    v = statistics.median(vals)
+    cb["value"] = v
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded pulsar + AWGN)",
+            "config": workload_config(samples, args.dms, ws), "cpu_baseline": cb,
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_reference_gpu(args):
+    ws, rank, _ = dist_setup()
+    if rank != 0:
+        return
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    if not os.path.exists(O.REF_GPU_RUNNER):
+        print(json.dumps({"impl": "reference-gpu", "unavailable": "oracle/_ref/ref_gpu_runner not built"}))
+        return
+    from msosm_gpu_b200 import simulate as S
+    samples = 1 << args.log2_samples
+    # the reference leaves delays uninitialised at DM 0: trials (0, 100]
+    dms = ((np.arange(args.dms) + 1) * DM_MAX / args.dms).astype(np.float32)
+    x = make_signal(samples)
+    u = S.quantise_uint16(x, 1000.0)
+    count = 32
+    ncalls = samples // (count * FFTPOINT // 2)
+    with tempfile.TemporaryDirectory() as td:
+        fin, fout = os.path.join(td, "in.u16"), os.path.join(td, "out.bin")
+        u.tofile(fin)
+        res = {}
+        for with_out in (0, 1):
+            cmd = [O.REF_GPU_RUNNER, "time", str(FFTPOINT), str(count), str(ncalls), str(max(args.steps, 1)),
+                   str(with_out), str(BW), str(F0), fin, fout] + [repr(float(v)) for v in dms]
+            r = subprocess.run(cmd, capture_output=True, text=True, timeout=1800)
+            if r.returncode != 0:
+                print(json.dumps({"impl": "reference-gpu", "unavailable": f"runner exit {r.returncode}: "
+                                  f"{r.stderr[-300:]}"}))
+                return
+            ms = O.read_records(fout)["ms"]
+            res[with_out] = float(np.median(ms))
+    units = float(args.dms) * samples
+    print(json.dumps({"impl": "reference-gpu", "metric": METRIC, "unit": UNIT,
+                      "value": units / (res[0] * 1e-3) / 1e6,
+                      "value_with_series_d2h": units / (res[1] * 1e-3) / 1e6,
+                      "ms_per_step": res[0], "ms_per_step_with_series_d2h": res[1], "steps": args.steps,
+                      "config": dict(workload_config(samples, args.dms, 1), dm_range_per_gpu=[float(dms[0]), DM_MAX],
+                                     count=count, input="uint16 offset binary (the reference API)"),
+                      "method": "reference MSOSM_GPU_DM_concurrent (cuFFT + its kernels, sm_100a), "
+                                "std::chrono around filter_block_uint16 loop + synchronize, pinned host input "
+                                "(its own drivers' method); no folding (the reference has none for this class)"}),
+          flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference-gpu"])
+    ap.add_argument("--log2-samples", type=int, default=LOG2_SAMPLES)
+    ap.add_argument("--dms", type=int, default=N_DM)
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    elif args.impl == "reference-gpu":
+        run_reference_gpu(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

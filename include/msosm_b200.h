@@ -1,0 +1,222 @@
+/*
+ * msosm_b200.h -- C ABI of the B200 (sm_100a) coherent-dedispersion library.
+ *
+ * Drop-in boundary for the hot path of msosm_gpu: MS-OSM (multi-segment
+ * overlap-save) and OSM coherent dedispersion of complex baseband for one or
+ * many DM trials, detection and phase folding.  Plain C types only; every
+ * entry point returns an msosm_status (0 = OK) and never exits the process.
+ * The reference interface each entry point replaces is cited beside it
+ * (paths inside the msosm_gpu tree).
+ *
+ * Memory: a handle owns its device buffers.  Input/output pointers may be
+ * host (pageable or pinned) or device pointers; host pointers are copied
+ * inside the call.  Calls on one handle are stream-ordered on the handle's
+ * stream; a handle is not thread-safe (one host thread per handle).
+ */
+#ifndef MSOSM_B200_H
+#define MSOSM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define MSOSM_API __attribute__((visibility("default")))
+#else
+#define MSOSM_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (the reference prints and calls exit(1) instead:
+ *      gpu/include/gpu_common.cuh:41-61) ---------------------------------- */
+typedef int msosm_status;
+#define MSOSM_OK 0
+#define MSOSM_ERR_BAD_ARG 1     /* invalid parameter or size */
+#define MSOSM_ERR_OOM 2         /* device allocation failed */
+#define MSOSM_ERR_CUDA 3        /* CUDA runtime error (message via msosm_last_error) */
+#define MSOSM_ERR_TIMEOUT 4     /* a bounded device wait expired */
+#define MSOSM_ERR_UNSUPPORTED 5 /* size/mode not built (e.g. FFT size outside 2^5..2^14) */
+#define MSOSM_ERR_STATE 6       /* call out of order (e.g. fold not configured) */
+#define MSOSM_ERR_NO_DEVICE 7   /* no CUDA device visible */
+
+/* Packed offset-binary sample pair, 0 = blank.
+ * Replaces `struct uint16_pair` (utils/include/globals.h:21-25). */
+typedef struct msosm_uint16_pair {
+    uint16_t first;
+    uint16_t second;
+} msosm_uint16_pair;
+
+/* Complex sample, layout of cufftComplex (utils/include/globals.h:28). */
+typedef struct msosm_complex {
+    float x;
+    float y;
+} msosm_complex;
+
+/* Thread-local message for the last non-OK status of this thread. */
+MSOSM_API const char *msosm_last_error(void);
+/* Library version, major*10000 + minor*100 + patch. */
+MSOSM_API int msosm_version(void);
+/* Number of CUDA devices (0 on a machine without a GPU; never fails). */
+MSOSM_API int msosm_device_count(void);
+
+/* ======================================================================
+ * Filter design and segmentation (host math, reference L3)
+ * ====================================================================== */
+
+/* Dispersion smear in samples: floor(kdm*dm*(1/f0^2-1/(f0+bw)^2)*fs), fs=bw,
+ * kdm=4.15e15, f0 = lower band edge in Hz.  dm <= 0 gives 0.
+ * Replaces Prepare_MSOSM::Prepare_MSOSM (dedispersion/msosm/msosm_prepare.cpp:3-15). */
+MSOSM_API msosm_status msosm_prepare_nd(float bw, float dm, float f0, unsigned long *Nd);
+
+/* MS-OSM minimum filter order 2^ceil(log2(2*sqrt(Nd))).
+ * Replaces Prepare_MSOSM::calculate_min_order (msosm_prepare.cpp:17-30). */
+MSOSM_API msosm_status msosm_prepare_min_order_msosm(unsigned long Nd, unsigned long *M_min);
+
+/* OSM minimum filter order 2*next_power_of_2(Nd).
+ * Replaces Prepare_OSM::calculate_min_order (dedispersion/overlap_save/osm_prepare.cpp:17-30). */
+MSOSM_API msosm_status msosm_prepare_min_order_osm(unsigned long Nd, unsigned long *M_min);
+
+/* Per-bin block delays delay_points[2M] and their count.
+ * Replaces Prepare_MSOSM::segmentation (msosm_prepare.cpp:86-152).  Nd == 0
+ * (undefined in the reference) gives delaycount 0 and all delays 0. */
+MSOSM_API msosm_status msosm_prepare_segmentation(float bw, float dm, float f0, unsigned long M,
+                                        int *delaycount, int *delay_points);
+
+/* Dedispersion filter H[2M] exactly as the reference designs it (chirp phase
+ * in FP64 on the GPU, unnormalised M-point inverse DFT, zero pad, 2M-point
+ * DFT; the extra factor M of the reference is kept).  Needs a GPU.
+ * Replaces Prepare_MSOSM::generate_dedisp_params (msosm_prepare.cpp:37-84). */
+MSOSM_API msosm_status msosm_prepare_dedisp_params(float bw, float dm, float f0, unsigned long M,
+                                         msosm_complex *H);
+
+/* ======================================================================
+ * Dedisperser: N DM trials over one input stream
+ * ====================================================================== */
+
+typedef struct msosm_dedisp msosm_dedisp;
+
+/* flags for msosm_dedisp_create */
+#define MSOSM_FLAG_OSM 0x1u      /* classical overlap-save (OSM_GPU_*) instead of MS-OSM */
+#define MSOSM_FLAG_NO_SERIES 0x2u /* do not materialise the dedispersed series (fold only) */
+
+typedef struct msosm_dedisp_info {
+    unsigned long M;        /* hop / filter order; FFT size is 2M */
+    unsigned long fftpoint; /* 2M */
+    unsigned long M_min;    /* largest minimum order over the trials */
+    int count;              /* FFT blocks per filter call; a call takes count*M samples */
+    int numDMs;
+    int ring_slots;         /* spectrum history ring depth */
+    int max_delaycount;
+    unsigned int flags;
+    unsigned long long calls;       /* filter calls done */
+    unsigned long long device_bytes; /* device memory held by the handle */
+} msosm_dedisp_info;
+
+/* Create and initialise.  bw/dm/f0 are per-trial arrays of numDMs (f0 =
+ * lower band edge, Hz).  fftpoint 0 = minimum; a smaller-than-minimum FFT is
+ * raised to the minimum (the reference prints a warning and does the same).
+ * input_size != 0 sets count = input_size / M.  All trials must share bw and
+ * f0 (one input stream).  Replaces MSOSM_GPU_DM_concurrent::
+ * MSOSM_GPU_DM_concurrent + initialize_uint16
+ * (dedispersion/msosm_dm_concurrent/msosm_gpu_dm_concurrent.cpp:3-108);
+ * with numDMs == 1 MSOSM_GPU_BATCH (dedispersion/msosm/msosm_gpu_batch.cpp:10-49);
+ * with MSOSM_FLAG_OSM OSM_GPU_BATCH / OSM_GPU_DM_concurrent
+ * (dedispersion/overlap_save/osm_gpu_batch.cpp:19-92,
+ *  dedispersion/overlap_save_dm_concurrent/osm_gpu_dm_concurrent.cpp:15-75). */
+MSOSM_API msosm_status msosm_dedisp_create(const float *bw, const float *dm, const float *f0, int numDMs,
+                                 unsigned long fftpoint, int count, unsigned long input_size,
+                                 unsigned int flags, msosm_dedisp **out);
+MSOSM_API msosm_status msosm_dedisp_destroy(msosm_dedisp *d);
+MSOSM_API msosm_status msosm_dedisp_get_info(const msosm_dedisp *d, msosm_dedisp_info *info);
+
+/* Per-trial parameters as computed at create (arrays of numDMs). */
+MSOSM_API msosm_status msosm_dedisp_get_nd(const msosm_dedisp *d, unsigned long *Nd);
+MSOSM_API msosm_status msosm_dedisp_get_delaycount(const msosm_dedisp *d, int *delaycount);
+/* delay_points of trial i, 2M ints (Prepare_*::delay_points). */
+MSOSM_API msosm_status msosm_dedisp_get_delay_points(const msosm_dedisp *d, int i, int *delay_points);
+/* H of trial i, 2M complex, in the reference's scaling (Prepare_*::dedisp_params). */
+MSOSM_API msosm_status msosm_dedisp_get_dedisp_params(const msosm_dedisp *d, int i, msosm_complex *H);
+
+/* Run the CUDA stream of this handle (a cudaStream_t, 0 = the handle's own). */
+MSOSM_API msosm_status msosm_dedisp_set_stream(msosm_dedisp *d, void *stream);
+
+/* Dedisperse the next count*M samples (all trials).  Replaces
+ * filter_block_uint16 (msosm_gpu_dm_concurrent.cpp:119-151,
+ * msosm_gpu_batch.cpp:75-94, osm_gpu_batch.cpp:94-123).  The input is
+ * offset-binary (x == 0 is blank, else x - 32768). */
+MSOSM_API msosm_status msosm_dedisp_filter_block_uint16(msosm_dedisp *d, const msosm_uint16_pair *input);
+/* Same for complex64 input (the reference has no such entry point). */
+MSOSM_API msosm_status msosm_dedisp_filter_block_c64(msosm_dedisp *d, const msosm_complex *input);
+
+/* Copy the dedispersed series of the last call: numDMs*count*M + 1 elements,
+ * layout [dm][count*M] plus a trailing zero element, as the reference.
+ * Scaling is the reference's (half the normalised convolution).  Blocks
+ * until the copy is done.  Replaces get_output(Complex*)
+ * (msosm_gpu_dm_concurrent.cpp:153-165, msosm_gpu_batch.cpp:96-99). */
+MSOSM_API msosm_status msosm_dedisp_get_output_c64(msosm_dedisp *d, msosm_complex *out);
+/* Same, requantised to offset-binary (v + 32768 truncated, 0 stays 0,
+ * saturating).  Replaces get_output(uint16_pair*) (:167-180) with
+ * complexToUint16 (gpu/gpu_kernel.cu:317-329). */
+MSOSM_API msosm_status msosm_dedisp_get_output_uint16(msosm_dedisp *d, msosm_uint16_pair *out);
+/* Device pointer of the series of the last call ([dm][count*M], complex). */
+MSOSM_API msosm_status msosm_dedisp_output_device_ptr(msosm_dedisp *d, msosm_complex **ptr);
+
+/* ---- fused detection + folding ------------------------------------------
+ * Folding follows Fold_GPU (folding/fold_gpu.cpp:3-194): period_samples =
+ * (unsigned long)(period*fs), one sample skipped whenever the float drift
+ * exceeds 1, the first ceil(discard_Nd/(period*fs)) periods discarded, only
+ * complete periods folded, then averaged into time_bin bins of
+ * period_samples/time_bin samples (tail dropped).  time_bin 0 keeps
+ * period_samples bins (no averaging).  Detection per sample: */
+#define MSOSM_DETECT_POWER 0     /* |y|^2 */
+#define MSOSM_DETECT_AMPLITUDE 1 /* |y|, the reference's calculateIntensity with one pol */
+MSOSM_API msosm_status msosm_dedisp_fold_init(msosm_dedisp *d, float period, float fs, unsigned long time_bin,
+                                    unsigned long discard_Nd, int detect);
+/* Folded profiles so far, numDMs x time_bin floats (fold_data_bins). */
+MSOSM_API msosm_status msosm_dedisp_get_profiles(msosm_dedisp *d, float *out);
+/* Number of whole periods folded so far. */
+MSOSM_API msosm_status msosm_dedisp_folded_periods(const msosm_dedisp *d, unsigned long long *n);
+
+/* Wait for all work of the handle (MSOSM_GPU_DM_concurrent::synchronize). */
+MSOSM_API msosm_status msosm_dedisp_synchronize(msosm_dedisp *d);
+
+/* ---- per-stage device timing -------------------------------------------
+ * CUDA events recorded on the handle's stream around each stage of every
+ * filter call (no effect on results).  Enabling resets the counters;
+ * msosm_dedisp_get_timing waits for the handle's work and sums. */
+typedef struct msosm_timing {
+    double forward_ms;  /* decode + forward FFT into the spectrum ring */
+    double dedisp_ms;   /* fused gather x H, inverse FFT, discard, detect, fold */
+    double fold_ms;     /* fold bookkeeping: partial-row clears, ordered reduce, flush */
+    double h2d_ms;      /* host-to-device input staging (copy stream) */
+    unsigned long long calls;           /* filter calls timed */
+    unsigned long long kernel_launches; /* kernels of this library launched by those calls */
+} msosm_timing;
+MSOSM_API msosm_status msosm_dedisp_enable_timing(msosm_dedisp *d, int on);
+MSOSM_API msosm_status msosm_dedisp_get_timing(msosm_dedisp *d, msosm_timing *t);
+
+/* ======================================================================
+ * Introspection for tests (host only, no GPU needed)
+ * ====================================================================== */
+
+/* Destination of every output sample of one fold chunk under the Fold_GPU
+ * state machine (folding/fold_gpu.cpp:48-173), as the device fold uses it:
+ * dest[i] = -1 if sample i is not folded (skipped by the drift, discarded, or
+ * in a period processed before the fold became ready), else
+ * (period_index << 32) | phase, phase in [0, period_samples).  A period only
+ * counts once all its period_samples samples have been seen.  The state
+ * carries across chunks through the planner handle; *completed returns the
+ * number of whole periods folded so far. */
+typedef struct msosm_fold_planner msosm_fold_planner;
+MSOSM_API msosm_status msosm_fold_planner_create(float period, float fs, unsigned long discard_Nd,
+                                       msosm_fold_planner **out);
+MSOSM_API msosm_status msosm_fold_planner_destroy(msosm_fold_planner *p);
+MSOSM_API msosm_status msosm_fold_planner_chunk(msosm_fold_planner *p, unsigned long size, int64_t *dest,
+                                      unsigned long long *completed);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MSOSM_B200_H */

@@ -1,0 +1,871 @@
+// api.cu -- the C ABI (include/msosm_b200.h) over the sm_100a kernels.
+#include "msosm_b200.h"
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "host_prepare.hpp"
+#include "kernels.hpp"
+
+using namespace msosm;
+
+namespace {
+
+thread_local std::string g_err;
+
+msosm_status fail(msosm_status s, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return s;
+}
+
+msosm_status cuda_fail(cudaError_t e, const char *what)
+{
+    cudaGetLastError();  // clear a non-sticky error
+    if (e == cudaErrorMemoryAllocation)
+        return fail(MSOSM_ERR_OOM, "%s: %s", what, cudaGetErrorString(e));
+    if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver)
+        return fail(MSOSM_ERR_NO_DEVICE, "%s: %s", what, cudaGetErrorString(e));
+    return fail(MSOSM_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define CK(call)                                                                                       \
+    do {                                                                                               \
+        cudaError_t e_ = (call);                                                                       \
+        if (e_ != cudaSuccess)                                                                         \
+            return cuda_fail(e_, #call);                                                               \
+    } while (0)
+
+int ilog2_exact(unsigned long n)
+{
+    if (n == 0 || (n & (n - 1)) != 0)
+        return -1;
+    int l = 0;
+    while ((1ul << l) < n)
+        ++l;
+    return l;
+}
+
+bool is_device_ptr(const void *p)
+{
+    cudaPointerAttributes at;
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+}
+
+// exp(sign * 2 pi i e / n), e < n, computed in double on the host
+std::vector<float2> twiddle_table(int n, int sign)
+{
+    std::vector<float2> t(n);
+    for (int e = 0; e < n; ++e) {
+        const double a = sign * 2.0 * kPi * (double)e / (double)n;
+        t[e] = make_float2((float)std::cos(a), (float)std::sin(a));
+    }
+    return t;
+}
+
+template <typename T>
+cudaError_t dalloc(T **p, size_t count, size_t &total)
+{
+    total += count * sizeof(T);
+    return cudaMalloc((void **)p, count * sizeof(T) + 16);
+}
+
+}  // namespace
+
+struct msosm_dedisp {
+    // configuration
+    int D = 0, count = 0, log2n = 0, S = 0, R = 1, grid = 1, max_dc = 0, max_delay = 0;
+    unsigned long M = 0, N = 0, M_min = 0;
+    unsigned int flags = 0;
+    bool series = true;
+    std::vector<unsigned long> Nd;
+    std::vector<int> dc;
+    std::vector<int> delays;  // D x N (host copy)
+    unsigned long long calls = 0;
+    size_t device_bytes = 0;
+    // streams and events
+    cudaStream_t stream = nullptr, own_stream = nullptr, copy_stream = nullptr;
+    cudaEvent_t ev_copied[2] = {nullptr, nullptr}, ev_consumed[2] = {nullptr, nullptr};
+    cudaEvent_t ev_spans[2] = {nullptr, nullptr};
+    // device buffers
+    float2 *ring = nullptr, *H = nullptr, *hist = nullptr, *series_buf = nullptr;
+    uint16_t *delays_d = nullptr;
+    float2 *tw_fwd = nullptr, *tw_inv = nullptr, *tw_inv_m = nullptr;
+    void *staging[2] = {nullptr, nullptr};
+    uint32_t *u16_out = nullptr;
+    // folding
+    bool fold = false;
+    int detect = 0, nbins = 0, bpt = 1, span_cap = 0;
+    unsigned long ps = 0;
+    double out_scale = 1.0;
+    FoldPlanner *planner = nullptr;
+    std::vector<FoldSpan> spans;
+    float *part_main = nullptr, *part_pend = nullptr, *prof_out = nullptr;
+    double *acc_main = nullptr, *acc_pend = nullptr;
+    long long *span_a_d = nullptr, *span_b_d = nullptr;
+    int *span_p_d = nullptr, *span_dest_d = nullptr;
+    // pinned span staging: [2][cap] of a, b, phase0, dest
+    long long *span_host = nullptr;
+    // timing: events per timed call: e0 [forward] e1 [fold prep] e2 [dedisp] e3
+    // [fold reduce] e6; e4 [h2d] e5 on the copy stream
+    bool timing = false;
+    struct CallEvents {
+        cudaEvent_t e[7];
+        bool h2d;
+    };
+    std::vector<CallEvents> timed;
+    unsigned long long launches = 0, timed_launches = 0;
+};
+
+namespace {
+
+void release(msosm_dedisp *d)
+{
+    if (!d)
+        return;
+    if (d->stream)
+        cudaStreamSynchronize(d->stream);
+    if (d->copy_stream)
+        cudaStreamSynchronize(d->copy_stream);
+    void *bufs[] = {d->ring, d->H, d->hist, d->series_buf, d->delays_d, d->tw_fwd, d->tw_inv, d->tw_inv_m,
+                    d->staging[0], d->staging[1], d->u16_out, d->part_main, d->part_pend, d->prof_out,
+                    d->acc_main, d->acc_pend, d->span_a_d, d->span_b_d, d->span_p_d, d->span_dest_d};
+    for (void *p : bufs)
+        if (p)
+            cudaFree(p);
+    if (d->span_host)
+        cudaFreeHost(d->span_host);
+    for (int i = 0; i < 2; ++i) {
+        if (d->ev_copied[i])
+            cudaEventDestroy(d->ev_copied[i]);
+        if (d->ev_consumed[i])
+            cudaEventDestroy(d->ev_consumed[i]);
+        if (d->ev_spans[i])
+            cudaEventDestroy(d->ev_spans[i]);
+    }
+    for (auto &c : d->timed)
+        for (cudaEvent_t e : c.e)
+            cudaEventDestroy(e);
+    if (d->copy_stream)
+        cudaStreamDestroy(d->copy_stream);
+    if (d->own_stream)
+        cudaStreamDestroy(d->own_stream);
+    delete d->planner;
+    delete d;
+}
+
+msosm_status upload_table(float2 **dst, int n, int sign, size_t &total, cudaStream_t st)
+{
+    std::vector<float2> t = twiddle_table(n, sign);
+    CK(dalloc(dst, (size_t)n, total));
+    CK(cudaMemcpyAsync(*dst, t.data(), sizeof(float2) * n, cudaMemcpyHostToDevice, st));
+    CK(cudaStreamSynchronize(st));
+    return MSOSM_OK;
+}
+
+// H of every trial on the device: H_ref * scale into H[D][N]
+msosm_status design_filters(int log2n, const std::vector<ChirpParams> &cp, float scale, int sign,
+                            const float2 *tw_inv_m, const float2 *tw_fwd, float2 *H, cudaStream_t st)
+{
+    ChirpParams *cp_d = nullptr;
+    CK(cudaMalloc((void **)&cp_d, sizeof(ChirpParams) * cp.size()));
+    cudaError_t e = cudaMemcpyAsync(cp_d, cp.data(), sizeof(ChirpParams) * cp.size(), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) {
+        DesignArgs a;
+        a.chirp = cp_d;
+        a.D = (int)cp.size();
+        a.tw_inv_m = tw_inv_m;
+        a.tw_fwd_n = tw_fwd;
+        a.H = H;
+        a.scale = scale;
+        a.sign = sign;
+        e = launch_design(log2n, a, st);
+    }
+    if (e == cudaSuccess)
+        e = cudaStreamSynchronize(st);
+    cudaFree(cp_d);
+    if (e != cudaSuccess)
+        return cuda_fail(e, "filter design");
+    return MSOSM_OK;
+}
+
+msosm_status check_handle(const msosm_dedisp *d)
+{
+    if (!d)
+        return fail(MSOSM_ERR_BAD_ARG, "null handle");
+    return MSOSM_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C ABI
+// ===========================================================================
+
+extern "C" {
+
+const char *msosm_last_error(void) { return g_err.c_str(); }
+int msosm_version(void) { return 100; }
+
+int msosm_device_count(void)
+{
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+msosm_status msosm_prepare_nd(float bw, float dm, float f0, unsigned long *Nd)
+{
+    if (!Nd || !(bw > 0) || !(f0 > 0))
+        return fail(MSOSM_ERR_BAD_ARG, "msosm_prepare_nd: bw and f0 must be positive");
+    *Nd = dispersion_smear(bw, dm, f0);
+    return MSOSM_OK;
+}
+
+msosm_status msosm_prepare_min_order_msosm(unsigned long Nd, unsigned long *M_min)
+{
+    if (!M_min)
+        return fail(MSOSM_ERR_BAD_ARG, "null output");
+    *M_min = msosm_min_order(Nd);
+    return MSOSM_OK;
+}
+
+msosm_status msosm_prepare_min_order_osm(unsigned long Nd, unsigned long *M_min)
+{
+    if (!M_min)
+        return fail(MSOSM_ERR_BAD_ARG, "null output");
+    *M_min = osm_min_order(Nd);
+    return MSOSM_OK;
+}
+
+msosm_status msosm_prepare_segmentation(float bw, float dm, float f0, unsigned long M, int *delaycount,
+                                        int *delay_points)
+{
+    if (!delaycount || !delay_points || M == 0 || !(bw > 0) || !(f0 > 0))
+        return fail(MSOSM_ERR_BAD_ARG, "msosm_prepare_segmentation: bad arguments");
+    *delaycount = segment_delays(bw, dm, f0, dispersion_smear(bw, dm, f0), M, delay_points);
+    return MSOSM_OK;
+}
+
+msosm_status msosm_prepare_dedisp_params(float bw, float dm, float f0, unsigned long M, msosm_complex *H)
+{
+    if (!H || !(bw > 0) || !(f0 > 0))
+        return fail(MSOSM_ERR_BAD_ARG, "msosm_prepare_dedisp_params: bad arguments");
+    const int log2n = ilog2_exact(2 * M);
+    if (log2n < 0)
+        return fail(MSOSM_ERR_BAD_ARG, "M must be a power of two");
+    if (!log2n_supported(log2n))
+        return fail(MSOSM_ERR_UNSUPPORTED, "FFT size %lu outside 64..16384", 2 * M);
+    if (msosm_device_count() == 0)
+        return fail(MSOSM_ERR_NO_DEVICE, "no CUDA device");
+    size_t total = 0;
+    cudaStream_t st = nullptr;
+    float2 *tw_m = nullptr, *tw_n = nullptr, *Hd = nullptr;
+    msosm_status s = MSOSM_OK;
+    CK(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+    if ((s = upload_table(&tw_m, (int)M, +1, total, st)) == MSOSM_OK &&
+        (s = upload_table(&tw_n, (int)(2 * M), -1, total, st)) == MSOSM_OK) {
+        cudaError_t e = cudaMalloc((void **)&Hd, sizeof(float2) * 2 * M);
+        if (e != cudaSuccess) {
+            s = cuda_fail(e, "cudaMalloc");
+        } else {
+            std::vector<ChirpParams> cp(1, chirp_params(bw, dm, f0, M));
+            s = design_filters(log2n, cp, 1.0f, -1, tw_m, tw_n, Hd, st);
+            if (s == MSOSM_OK) {
+                e = cudaMemcpy(H, Hd, sizeof(float2) * 2 * M, cudaMemcpyDeviceToHost);
+                if (e != cudaSuccess)
+                    s = cuda_fail(e, "cudaMemcpy");
+            }
+        }
+    }
+    cudaFree(Hd);
+    cudaFree(tw_m);
+    cudaFree(tw_n);
+    cudaStreamDestroy(st);
+    return s;
+}
+
+msosm_status msosm_dedisp_create(const float *bw, const float *dm, const float *f0, int numDMs,
+                                 unsigned long fftpoint, int count, unsigned long input_size,
+                                 unsigned int flags, msosm_dedisp **out)
+{
+    if (!out || !bw || !dm || !f0 || numDMs < 1)
+        return fail(MSOSM_ERR_BAD_ARG, "msosm_dedisp_create: null argument or numDMs < 1");
+    *out = nullptr;
+    if (flags & ~(MSOSM_FLAG_OSM | MSOSM_FLAG_NO_SERIES))
+        return fail(MSOSM_ERR_BAD_ARG, "unknown flags 0x%x", flags);
+    for (int i = 0; i < numDMs; ++i)
+        if (!(bw[i] > 0) || !(f0[i] > 0) || !(dm[i] >= 0) || !std::isfinite(dm[i]))
+            return fail(MSOSM_ERR_BAD_ARG, "trial %d: bw, f0 must be > 0 and dm >= 0", i);
+    const bool osm = (flags & MSOSM_FLAG_OSM) != 0;
+    msosm_dedisp *d = new (std::nothrow) msosm_dedisp;
+    if (!d)
+        return fail(MSOSM_ERR_OOM, "host allocation");
+    d->D = numDMs;
+    d->flags = flags;
+    d->series = (flags & MSOSM_FLAG_NO_SERIES) == 0;
+    d->Nd.resize(numDMs);
+    d->dc.assign(numDMs, 0);
+    // minimum orders, common order (msosm_prepare_dm_concurrent.cpp:31-49,
+    // msosm_gpu_dm_concurrent.cpp:29-42)
+    unsigned long Mc = 0;
+    for (int i = 0; i < numDMs; ++i) {
+        d->Nd[i] = dispersion_smear(bw[i], dm[i], f0[i]);
+        const unsigned long m = osm ? osm_min_order(d->Nd[i]) : msosm_min_order(d->Nd[i]);
+        Mc = m > Mc ? m : Mc;
+    }
+    d->M_min = Mc;
+    unsigned long M = Mc;
+    if (fftpoint != 0) {
+        M = fftpoint / 2;
+        if (M < Mc)
+            M = Mc;  // the reference warns and raises the FFT to the minimum
+    }
+    const int log2n = ilog2_exact(2 * M);
+    if (log2n < 0) {
+        release(d);
+        return fail(MSOSM_ERR_BAD_ARG, "FFT size %lu is not a power of two", 2 * M);
+    }
+    if (!log2n_supported(log2n)) {
+        release(d);
+        return fail(MSOSM_ERR_UNSUPPORTED, "FFT size %lu outside the supported 64..16384", 2 * M);
+    }
+    if (input_size != 0)
+        count = (int)(input_size / M);
+    if (count < 1) {
+        release(d);
+        return fail(MSOSM_ERR_BAD_ARG, "count must be >= 1");
+    }
+    d->M = M;
+    d->N = 2 * M;
+    d->log2n = log2n;
+    d->count = count;
+    const unsigned long N = d->N;
+    d->delays.assign((size_t)numDMs * N, 0);
+    if (!osm) {
+        for (int i = 0; i < numDMs; ++i)
+            d->dc[i] = segment_delays(bw[i], dm[i], f0[i], d->Nd[i], M, d->delays.data() + (size_t)i * N);
+    }
+    for (int i = 0; i < numDMs; ++i) {
+        d->max_dc = d->dc[i] > d->max_dc ? d->dc[i] : d->max_dc;
+        for (unsigned long b = 0; b < N; ++b)
+            d->max_delay = d->delays[(size_t)i * N + b] > d->max_delay ? d->delays[(size_t)i * N + b] : d->max_delay;
+    }
+    if (d->max_delay > 65535) {
+        release(d);
+        return fail(MSOSM_ERR_UNSUPPORTED, "block delay %d exceeds 65535", d->max_delay);
+    }
+    if (msosm_device_count() == 0) {
+        release(d);
+        return fail(MSOSM_ERR_NO_DEVICE, "no CUDA device");
+    }
+    // spectra of blocks [k0 - max_delay, k0 + count) must be resident
+    d->S = count + d->max_delay;
+
+#define CKD(call)                                                                                      \
+    do {                                                                                               \
+        cudaError_t e_ = (call);                                                                       \
+        if (e_ != cudaSuccess) {                                                                       \
+            msosm_status s_ = cuda_fail(e_, #call);                                                    \
+            release(d);                                                                                \
+            return s_;                                                                                 \
+        }                                                                                              \
+    } while (0)
+
+    CKD(cudaStreamCreateWithFlags(&d->own_stream, cudaStreamNonBlocking));
+    CKD(cudaStreamCreateWithFlags(&d->copy_stream, cudaStreamNonBlocking));
+    d->stream = d->own_stream;
+    for (int i = 0; i < 2; ++i) {
+        CKD(cudaEventCreateWithFlags(&d->ev_copied[i], cudaEventDisableTiming));
+        CKD(cudaEventCreateWithFlags(&d->ev_consumed[i], cudaEventDisableTiming));
+        CKD(cudaEventCreateWithFlags(&d->ev_spans[i], cudaEventDisableTiming));
+    }
+    size_t &tot = d->device_bytes;
+    CKD(dalloc(&d->ring, (size_t)d->S * N, tot));
+    CKD(dalloc(&d->H, (size_t)numDMs * N, tot));
+    CKD(dalloc(&d->delays_d, (size_t)numDMs * N, tot));
+    CKD(dalloc(&d->hist, 2 * (size_t)M, tot));
+    CKD(cudaMemsetAsync(d->hist, 0, sizeof(float2) * 2 * M, d->stream));
+    for (int i = 0; i < 2; ++i)
+        CKD(dalloc((float2 **)&d->staging[i], (size_t)count * M, tot));
+    if (d->series)
+        CKD(dalloc(&d->series_buf, (size_t)numDMs * count * M + 1, tot));
+    {
+        std::vector<uint16_t> dl(d->delays.size());
+        for (size_t i = 0; i < dl.size(); ++i)
+            dl[i] = (uint16_t)d->delays[i];
+        CKD(cudaMemcpy(d->delays_d, dl.data(), sizeof(uint16_t) * dl.size(), cudaMemcpyHostToDevice));
+    }
+    msosm_status s;
+    if ((s = upload_table(&d->tw_fwd, (int)N, -1, tot, d->stream)) != MSOSM_OK ||
+        (s = upload_table(&d->tw_inv, (int)N, +1, tot, d->stream)) != MSOSM_OK ||
+        (s = upload_table(&d->tw_inv_m, (int)M, +1, tot, d->stream)) != MSOSM_OK) {
+        release(d);
+        return s;
+    }
+    std::vector<ChirpParams> cp(numDMs);
+    for (int i = 0; i < numDMs; ++i)
+        cp[i] = chirp_params(bw[i], dm[i], f0[i], M);
+    // 1/N^2: the reference's /N before and /(2M) after the inverse FFT
+    const float scale = 1.0f / ((float)N * (float)N);
+    if ((s = design_filters(log2n, cp, scale, -1, d->tw_inv_m, d->tw_fwd, d->H, d->stream)) != MSOSM_OK) {
+        release(d);
+        return s;
+    }
+    // persistent grid: work items (block range, trial), balanced over waves
+    int dev = 0, sms = 0;
+    CKD(cudaGetDevice(&dev));
+    CKD(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    int per_sm = dedisp_blocks_per_sm(log2n, d->series, false);
+    if (per_sm < 1)
+        per_sm = 1;
+    const long long resident = (long long)per_sm * sms;
+    long long R = (8 * resident + numDMs - 1) / numDMs;
+    if (R > count)
+        R = count;
+    if (R < 1)
+        R = 1;
+    d->R = (int)R;
+    const long long items = (long long)numDMs * R;
+    const long long waves = (items + resident - 1) / resident;
+    d->grid = (int)((items + waves - 1) / waves);
+#undef CKD
+    *out = d;
+    return MSOSM_OK;
+}
+
+msosm_status msosm_dedisp_destroy(msosm_dedisp *d)
+{
+    release(d);
+    return MSOSM_OK;
+}
+
+msosm_status msosm_dedisp_get_info(const msosm_dedisp *d, msosm_dedisp_info *info)
+{
+    if (check_handle(d) || !info)
+        return fail(MSOSM_ERR_BAD_ARG, "null argument");
+    info->M = d->M;
+    info->fftpoint = d->N;
+    info->M_min = d->M_min;
+    info->count = d->count;
+    info->numDMs = d->D;
+    info->ring_slots = d->S;
+    info->max_delaycount = d->max_dc;
+    info->flags = d->flags;
+    info->calls = d->calls;
+    info->device_bytes = d->device_bytes;
+    return MSOSM_OK;
+}
+
+msosm_status msosm_dedisp_get_nd(const msosm_dedisp *d, unsigned long *Nd)
+{
+    if (check_handle(d) || !Nd)
+        return fail(MSOSM_ERR_BAD_ARG, "null argument");
+    for (int i = 0; i < d->D; ++i)
+        Nd[i] = d->Nd[i];
+    return MSOSM_OK;
+}
+
+msosm_status msosm_dedisp_get_delaycount(const msosm_dedisp *d, int *dc)
+{
+    if (check_handle(d) || !dc)
+        return fail(MSOSM_ERR_BAD_ARG, "null argument");
+    for (int i = 0; i < d->D; ++i)
+        dc[i] = d->dc[i];
+    return MSOSM_OK;
+}
+
+msosm_status msosm_dedisp_get_delay_points(const msosm_dedisp *d, int i, int *dp)
+{
+    if (check_handle(d) || !dp || i < 0 || i >= d->D)
+        return fail(MSOSM_ERR_BAD_ARG, "bad trial index or null output");
+    std::memcpy(dp, d->delays.data() + (size_t)i * d->N, sizeof(int) * d->N);
+    return MSOSM_OK;
+}
+
+msosm_status msosm_dedisp_get_dedisp_params(const msosm_dedisp *d, int i, msosm_complex *H)
+{
+    if (check_handle(d) || !H || i < 0 || i >= d->D)
+        return fail(MSOSM_ERR_BAD_ARG, "bad trial index or null output");
+    CK(cudaStreamSynchronize(d->stream));
+    CK(cudaMemcpy(H, d->H + (size_t)i * d->N, sizeof(float2) * d->N, cudaMemcpyDeviceToHost));
+    const float up = (float)d->N * (float)d->N;  // undo the 1/N^2 (a power of two: exact)
+    for (unsigned long b = 0; b < d->N; ++b) {
+        H[b].x *= up;
+        H[b].y *= up;
+    }
+    return MSOSM_OK;
+}
+
+msosm_status msosm_dedisp_set_stream(msosm_dedisp *d, void *stream)
+{
+    if (check_handle(d))
+        return MSOSM_ERR_BAD_ARG;
+    CK(cudaStreamSynchronize(d->stream));
+    d->stream = stream ? (cudaStream_t)stream : d->own_stream;
+    return MSOSM_OK;
+}
+
+static msosm_status filter_block(msosm_dedisp *d, const void *input, InputKind kind)
+{
+    if (check_handle(d) || !input)
+        return fail(MSOSM_ERR_BAD_ARG, "null handle or input");
+    const size_t elem = kind == kInputU16 ? 4 : 8;
+    const size_t bytes = (size_t)d->count * d->M * elem;
+    const int sb = (int)(d->calls & 1);
+    const void *src = input;
+    msosm_dedisp::CallEvents *ev = nullptr;
+    if (d->timing) {
+        msosm_dedisp::CallEvents c{};
+        for (cudaEvent_t &e : c.e)
+            CK(cudaEventCreate(&e));
+        c.h2d = false;
+        d->timed.push_back(c);
+        ev = &d->timed.back();
+    }
+    const unsigned long long launches0 = d->launches;
+    if (!is_device_ptr(input)) {
+        // stage through a device buffer on the copy stream; the host buffer
+        // may be reused as soon as this call returns
+        CK(cudaStreamWaitEvent(d->copy_stream, d->ev_consumed[sb], 0));
+        if (ev) {
+            CK(cudaEventRecord(ev->e[4], d->copy_stream));
+            ev->h2d = true;
+        }
+        CK(cudaMemcpyAsync(d->staging[sb], input, bytes, cudaMemcpyHostToDevice, d->copy_stream));
+        if (ev)
+            CK(cudaEventRecord(ev->e[5], d->copy_stream));
+        CK(cudaEventRecord(d->ev_copied[sb], d->copy_stream));
+        CK(cudaEventSynchronize(d->ev_copied[sb]));
+        CK(cudaStreamWaitEvent(d->stream, d->ev_copied[sb], 0));
+        src = d->staging[sb];
+    }
+    FwdArgs fa;
+    fa.input = src;
+    fa.hist_in = d->hist + (size_t)(d->calls & 1) * d->M;
+    fa.hist_out = d->hist + (size_t)((d->calls + 1) & 1) * d->M;
+    fa.ring = d->ring;
+    fa.S = d->S;
+    fa.k0 = (long long)d->calls * d->count;
+    fa.count = d->count;
+    fa.tw = d->tw_fwd;
+    if (ev)
+        CK(cudaEventRecord(ev->e[0], d->stream));
+    CK(launch_forward(d->log2n, kind, fa, d->stream));
+    d->launches += 1;
+    CK(cudaEventRecord(d->ev_consumed[sb], d->stream));
+    if (ev)
+        CK(cudaEventRecord(ev->e[1], d->stream));
+
+    DedispArgs da;
+    da.ring = d->ring;
+    da.S = d->S;
+    da.k0 = fa.k0;
+    da.count = d->count;
+    da.D = d->D;
+    da.R = d->R;
+    da.H = d->H;
+    da.delays = d->delays_d;
+    da.tw = d->tw_inv;
+    da.series = d->series_buf;
+    da.fold.nspans = -1;
+    if (d->fold) {
+        bool flush = false;
+        d->planner->chunk((unsigned long)d->count * d->M, d->spans, flush);
+        const int n = (int)d->spans.size();
+        if (n > d->span_cap)
+            return fail(MSOSM_ERR_STATE, "fold planner produced %d spans (capacity %d)", n, d->span_cap);
+        // reuse of the pinned span staging: wait for its copy two calls ago
+        CK(cudaEventSynchronize(d->ev_spans[sb]));
+        long long *h = d->span_host + (size_t)sb * 4 * d->span_cap;
+        for (int i = 0; i < n; ++i) {
+            h[i] = d->spans[i].a;
+            h[d->span_cap + i] = d->spans[i].b;
+            int *hp = reinterpret_cast<int *>(h + 2 * d->span_cap);
+            hp[i] = d->spans[i].phase0;
+            hp[d->span_cap + i] = d->spans[i].dest;
+        }
+        CK(cudaMemcpyAsync(d->span_a_d, h, sizeof(long long) * n, cudaMemcpyHostToDevice, d->stream));
+        CK(cudaMemcpyAsync(d->span_b_d, h + d->span_cap, sizeof(long long) * n, cudaMemcpyHostToDevice, d->stream));
+        const int *hp = reinterpret_cast<const int *>(h + 2 * d->span_cap);
+        CK(cudaMemcpyAsync(d->span_p_d, hp, sizeof(int) * n, cudaMemcpyHostToDevice, d->stream));
+        CK(cudaMemcpyAsync(d->span_dest_d, hp + d->span_cap, sizeof(int) * n, cudaMemcpyHostToDevice, d->stream));
+        CK(cudaEventRecord(d->ev_spans[sb], d->stream));
+        if (flush) {
+            CK(launch_fold_flush(d->acc_main, d->acc_pend, (size_t)d->D * d->nbins, d->stream));
+            d->launches += 1;
+        }
+        const size_t prow = (size_t)d->D * d->R * d->nbins;
+        CK(cudaMemsetAsync(d->part_main, 0, sizeof(float) * prow, d->stream));
+        CK(cudaMemsetAsync(d->part_pend, 0, sizeof(float) * prow, d->stream));
+        da.fold.span_a = d->span_a_d;
+        da.fold.span_b = d->span_b_d;
+        da.fold.span_phase0 = d->span_p_d;
+        da.fold.span_dest = d->span_dest_d;
+        da.fold.nspans = n;
+        da.fold.bpt = d->bpt;
+        da.fold.nbins = d->nbins;
+        da.fold.detect = d->detect;
+        da.fold.part_main = d->part_main;
+        da.fold.part_pend = d->part_pend;
+    }
+    // the partial-row clears and the flush above belong to the fold time;
+    // the dedispersion kernel is timed alone
+    if (ev)
+        CK(cudaEventRecord(ev->e[2], d->stream));
+    CK(launch_dedisp(d->log2n, d->series, d->fold, da, d->grid, d->stream));
+    d->launches += 1;
+    if (ev)
+        CK(cudaEventRecord(ev->e[3], d->stream));
+    if (d->fold) {
+        CK(launch_fold_reduce(d->part_main, d->part_pend, d->D, d->R, d->nbins, d->acc_main, d->acc_pend,
+                              d->stream));
+        d->launches += 1;
+    }
+    if (d->series)
+        CK(cudaMemsetAsync(d->series_buf + (size_t)d->D * d->count * d->M, 0, sizeof(float2), d->stream));
+    if (ev) {
+        CK(cudaEventRecord(ev->e[6], d->stream));
+        d->timed_launches += d->launches - launches0;
+    }
+    d->calls += 1;
+    return MSOSM_OK;
+}
+
+msosm_status msosm_dedisp_filter_block_uint16(msosm_dedisp *d, const msosm_uint16_pair *input)
+{
+    return filter_block(d, input, kInputU16);
+}
+
+msosm_status msosm_dedisp_filter_block_c64(msosm_dedisp *d, const msosm_complex *input)
+{
+    return filter_block(d, input, kInputC64);
+}
+
+msosm_status msosm_dedisp_get_output_c64(msosm_dedisp *d, msosm_complex *out)
+{
+    if (check_handle(d) || !out)
+        return fail(MSOSM_ERR_BAD_ARG, "null argument");
+    if (!d->series)
+        return fail(MSOSM_ERR_STATE, "handle created with MSOSM_FLAG_NO_SERIES");
+    const size_t n = (size_t)d->D * d->count * d->M + 1;
+    CK(cudaMemcpyAsync(out, d->series_buf, sizeof(float2) * n, cudaMemcpyDeviceToHost, d->stream));
+    CK(cudaStreamSynchronize(d->stream));
+    return MSOSM_OK;
+}
+
+msosm_status msosm_dedisp_get_output_uint16(msosm_dedisp *d, msosm_uint16_pair *out)
+{
+    if (check_handle(d) || !out)
+        return fail(MSOSM_ERR_BAD_ARG, "null argument");
+    if (!d->series)
+        return fail(MSOSM_ERR_STATE, "handle created with MSOSM_FLAG_NO_SERIES");
+    const size_t n = (size_t)d->D * d->count * d->M + 1;
+    if (!d->u16_out)
+        CK(dalloc(&d->u16_out, n, d->device_bytes));
+    CK(launch_encode_u16(d->series_buf, d->u16_out, n, d->stream));
+    CK(cudaMemcpyAsync(out, d->u16_out, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, d->stream));
+    CK(cudaStreamSynchronize(d->stream));
+    return MSOSM_OK;
+}
+
+msosm_status msosm_dedisp_output_device_ptr(msosm_dedisp *d, msosm_complex **ptr)
+{
+    if (check_handle(d) || !ptr)
+        return fail(MSOSM_ERR_BAD_ARG, "null argument");
+    *ptr = reinterpret_cast<msosm_complex *>(d->series_buf);
+    return d->series ? MSOSM_OK : fail(MSOSM_ERR_STATE, "handle created with MSOSM_FLAG_NO_SERIES");
+}
+
+msosm_status msosm_dedisp_fold_init(msosm_dedisp *d, float period, float fs, unsigned long time_bin,
+                                    unsigned long discard_Nd, int detect)
+{
+    if (check_handle(d))
+        return MSOSM_ERR_BAD_ARG;
+    if (d->fold)
+        return fail(MSOSM_ERR_STATE, "fold already configured");
+    if (detect != MSOSM_DETECT_POWER && detect != MSOSM_DETECT_AMPLITUDE)
+        return fail(MSOSM_ERR_BAD_ARG, "unknown detection %d", detect);
+    if (!(period > 0) || !(fs > 0))
+        return fail(MSOSM_ERR_BAD_ARG, "period and fs must be positive");
+    FoldPlanner *p = new (std::nothrow) FoldPlanner(period, fs, discard_Nd, true);
+    if (!p)
+        return fail(MSOSM_ERR_OOM, "host allocation");
+    const unsigned long ps = p->period_samples();
+    if (ps == 0 || ps > (1ul << 30)) {
+        delete p;
+        return fail(MSOSM_ERR_BAD_ARG, "period*fs gives %lu samples", ps);
+    }
+    const unsigned long nb = time_bin == 0 ? ps : time_bin;
+    if (nb > ps) {
+        delete p;
+        return fail(MSOSM_ERR_BAD_ARG, "time_bin %lu exceeds period_samples %lu", time_bin, ps);
+    }
+    d->planner = p;
+    d->ps = ps;
+    d->nbins = (int)nb;
+    d->bpt = nb == ps ? 1 : (int)(ps / nb);
+    d->out_scale = nb == ps ? 1.0 : 1.0 / (double)d->bpt;
+    d->detect = detect;
+    d->span_cap = (int)((unsigned long)d->count * d->M / ps) + 8;
+    size_t &tot = d->device_bytes;
+    const size_t prow = (size_t)d->D * d->R * d->nbins;
+    const size_t nacc = (size_t)d->D * d->nbins;
+    CK(dalloc(&d->part_main, prow, tot));
+    CK(dalloc(&d->part_pend, prow, tot));
+    CK(dalloc(&d->acc_main, nacc, tot));
+    CK(dalloc(&d->acc_pend, nacc, tot));
+    CK(dalloc(&d->prof_out, nacc, tot));
+    CK(dalloc(&d->span_a_d, (size_t)d->span_cap, tot));
+    CK(dalloc(&d->span_b_d, (size_t)d->span_cap, tot));
+    CK(dalloc(&d->span_p_d, (size_t)d->span_cap, tot));
+    CK(dalloc(&d->span_dest_d, (size_t)d->span_cap, tot));
+    CK(cudaMallocHost((void **)&d->span_host, sizeof(long long) * 2 * 4 * d->span_cap));
+    CK(cudaMemsetAsync(d->acc_main, 0, sizeof(double) * nacc, d->stream));
+    CK(cudaMemsetAsync(d->acc_pend, 0, sizeof(double) * nacc, d->stream));
+    CK(cudaStreamSynchronize(d->stream));
+    d->fold = true;
+    return MSOSM_OK;
+}
+
+msosm_status msosm_dedisp_get_profiles(msosm_dedisp *d, float *out)
+{
+    if (check_handle(d) || !out)
+        return fail(MSOSM_ERR_BAD_ARG, "null argument");
+    if (!d->fold)
+        return fail(MSOSM_ERR_STATE, "fold not configured (msosm_dedisp_fold_init)");
+    const size_t n = (size_t)d->D * d->nbins;
+    CK(launch_fold_readout(d->acc_main, n, d->out_scale, d->prof_out, d->stream));
+    CK(cudaMemcpyAsync(out, d->prof_out, sizeof(float) * n, cudaMemcpyDeviceToHost, d->stream));
+    CK(cudaStreamSynchronize(d->stream));
+    return MSOSM_OK;
+}
+
+msosm_status msosm_dedisp_folded_periods(const msosm_dedisp *d, unsigned long long *n)
+{
+    if (check_handle(d) || !n)
+        return fail(MSOSM_ERR_BAD_ARG, "null argument");
+    *n = d->planner ? d->planner->completed_folded() : 0;
+    return MSOSM_OK;
+}
+
+msosm_status msosm_dedisp_synchronize(msosm_dedisp *d)
+{
+    if (check_handle(d))
+        return MSOSM_ERR_BAD_ARG;
+    CK(cudaStreamSynchronize(d->stream));
+    CK(cudaStreamSynchronize(d->copy_stream));
+    return MSOSM_OK;
+}
+
+msosm_status msosm_dedisp_enable_timing(msosm_dedisp *d, int on)
+{
+    if (check_handle(d))
+        return MSOSM_ERR_BAD_ARG;
+    CK(cudaStreamSynchronize(d->stream));
+    for (auto &c : d->timed)
+        for (cudaEvent_t e : c.e)
+            cudaEventDestroy(e);
+    d->timed.clear();
+    d->timed_launches = 0;
+    d->timing = on != 0;
+    return MSOSM_OK;
+}
+
+msosm_status msosm_dedisp_get_timing(msosm_dedisp *d, msosm_timing *t)
+{
+    if (check_handle(d) || !t)
+        return fail(MSOSM_ERR_BAD_ARG, "null argument");
+    CK(cudaStreamSynchronize(d->stream));
+    CK(cudaStreamSynchronize(d->copy_stream));
+    std::memset(t, 0, sizeof *t);
+    for (auto &c : d->timed) {
+        float a = 0, b = 0, f = 0, g = 0, h = 0;
+        CK(cudaEventElapsedTime(&a, c.e[0], c.e[1]));
+        CK(cudaEventElapsedTime(&b, c.e[2], c.e[3]));
+        CK(cudaEventElapsedTime(&f, c.e[1], c.e[2]));
+        CK(cudaEventElapsedTime(&g, c.e[3], c.e[6]));
+        t->forward_ms += a;
+        t->dedisp_ms += b;
+        t->fold_ms += f + g;
+        if (c.h2d) {
+            CK(cudaEventElapsedTime(&h, c.e[4], c.e[5]));
+            t->h2d_ms += h;
+        }
+    }
+    t->calls = d->timed.size();
+    t->kernel_launches = d->timed_launches;
+    return MSOSM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// fold planner introspection
+// ---------------------------------------------------------------------------
+
+struct msosm_fold_planner {
+    FoldPlanner p;
+    std::vector<FoldSpan> spans;
+    msosm_fold_planner(float period, float fs, unsigned long nd) : p(period, fs, nd, true) {}
+};
+
+msosm_status msosm_fold_planner_create(float period, float fs, unsigned long discard_Nd, msosm_fold_planner **out)
+{
+    if (!out || !(period > 0) || !(fs > 0))
+        return fail(MSOSM_ERR_BAD_ARG, "bad arguments");
+    *out = new (std::nothrow) msosm_fold_planner(period, fs, discard_Nd);
+    if (!*out)
+        return fail(MSOSM_ERR_OOM, "host allocation");
+    if ((*out)->p.period_samples() == 0) {
+        delete *out;
+        *out = nullptr;
+        return fail(MSOSM_ERR_BAD_ARG, "period*fs < 1 sample");
+    }
+    return MSOSM_OK;
+}
+
+msosm_status msosm_fold_planner_destroy(msosm_fold_planner *p)
+{
+    delete p;
+    return MSOSM_OK;
+}
+
+msosm_status msosm_fold_planner_chunk(msosm_fold_planner *p, unsigned long size, int64_t *dest,
+                                      unsigned long long *completed)
+{
+    if (!p || !dest)
+        return fail(MSOSM_ERR_BAD_ARG, "null argument");
+    bool flush = false;
+    p->p.chunk(size, p->spans, flush);
+    for (unsigned long i = 0; i < size; ++i)
+        dest[i] = -1;
+    for (const FoldSpan &s : p->spans) {
+        if (s.dest == 0)
+            continue;
+        for (int64_t t = s.a; t < s.b; ++t)
+            dest[t] = (s.period << 32) | (int64_t)(s.phase0 + (t - s.a));
+    }
+    if (completed)
+        *completed = p->p.completed_folded();
+    return MSOSM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,527 @@
+// kernels.cu -- sm_100a kernels of the MS-OSM / OSM dedispersion path.
+//
+//   forward_kernel  decode (uint16 offset-binary or complex64) + forward FFT of
+//                   the overlapping windows of one call, written into the
+//                   spectrum ring shared by all DM trials.  Replaces
+//                   uint16ToComplex + the forward cufftExecC2C
+//                   (gpu/gpu_kernel.cu:276-299, msosm_gpu_dm_concurrent.cpp:123-129).
+//   dedisp_kernel   persistent; per (DM trial, block): gather each bin's
+//                   delayed spectrum from the ring, multiply by H, inverse FFT
+//                   in shared memory, keep the second half (overlap-save
+//                   discard), then write the series and/or detect and fold.
+//                   Replaces ComplexMultiplyDelay_concurrent_batch + inverse
+//                   cufftExecC2C + DiscardSamples_concurrent_batch
+//                   (gpu/gpu_kernel.cu:128-198,236-258) and, fused, the
+//                   calculateIntensity kernel + host fold of Fold_GPU
+//                   (gpu/gpu_kernel.cu:347-353, folding/fold_gpu.cpp:48-194).
+//   design_kernel   dedispersion filter H per trial on the device: FP64 chirp
+//                   phase reduced mod 2 pi, M-point inverse FFT, zero pad,
+//                   2M-point FFT (msosm_prepare.cpp:37-84 on the host in the
+//                   reference).
+//
+// Ring semantics: the reference scatters X[c][b]*H[b]/N into a per-DM product
+// ring at slot (index + c + delay[b]) % S and inverse-transforms slots
+// index..index+count-1 (gpu/gpu_kernel.cu:179-184).  A slot therefore holds,
+// for bin b, the product of block k - delay[b] (zero before the stream
+// start).  Here the ring holds the input spectra once for all trials and
+// each trial gathers X[k - delay[b]][b] * H[b] directly.
+#include "fft_smem.cuh"
+#include "kernels.hpp"
+
+#include <cuda_runtime.h>
+
+namespace msosm {
+
+// ---------------------------------------------------------------------------
+// forward transform of the input windows
+// ---------------------------------------------------------------------------
+
+template <int KIND>
+__device__ __forceinline__ float2 load_sample(const void *p, long long s)
+{
+    if constexpr (KIND == kInputC64) {
+        return reinterpret_cast<const float2 *>(p)[s];
+    } else {
+        // offset binary, 0 = blank (gpu/gpu_kernel.cu:291-296)
+        const uint32_t u = reinterpret_cast<const uint32_t *>(p)[s];
+        const uint32_t x = u & 0xFFFFu, y = u >> 16;
+        return make_float2(x ? (float)x - 32768.0f : 0.0f, y ? (float)y - 32768.0f : 0.0f);
+    }
+}
+
+template <int LOG2N, int KIND, bool PP>
+__global__ void __launch_bounds__(FftShape<LOG2N>::T) forward_kernel(FwdArgs a)
+{
+    using F = FftShape<LOG2N>;
+    constexpr int N = F::N, M = N / 2, T = F::T;
+    extern __shared__ float2 smem[];
+    float2 *buf0 = smem;
+    float2 *buf1 = PP ? smem + F::SMEM : smem;
+    const int tid = threadIdx.x;
+    const int c = blockIdx.x;
+    float2 v[16];
+    // window c covers input samples [c*M - M, c*M + M); negative indices are
+    // the previous call's last M samples (the reference's D2D overlap copy,
+    // msosm_gpu_dm_concurrent.cpp:125)
+#pragma unroll
+    for (int r = 0; r < 16; ++r) {
+        const int n = tid + r * T;
+        const long long s = (long long)c * M + n - M;
+        const float2 x = (s < 0) ? a.hist_in[M + s] : load_sample<KIND>(a.input, s);
+        if (c == a.count - 1 && n >= M)
+            a.hist_out[n - M] = x;
+        v[r] = x;
+    }
+    dft16<-1>(v);
+    stage_store<LOG2N, 0>(v, buf0, tid);
+    run_stages<LOG2N, -1, PP>(v, buf0, buf1, tid, a.tw);
+    float2 *row = a.ring + (size_t)((a.k0 + c) % a.S) * N;
+#pragma unroll
+    for (int slot = 0; slot < 16; ++slot)
+        row[last_out_index<LOG2N>(tid, slot)] = v[slot];
+}
+
+// ---------------------------------------------------------------------------
+// fused dedispersion + detection + folding
+// ---------------------------------------------------------------------------
+
+// Fold the M intensities of one block (ibuf, chunk-local samples t0 ..
+// t0+M-1) into the work item's partial-profile rows.  Spans come from the
+// host fold planner (sorted, disjoint).  Every bin of one span is summed by
+// one thread in sample order; spans are separated by barriers, so a bin is
+// never updated by two threads at once and the result does not depend on
+// scheduling.
+__device__ __forceinline__ void fold_block(const FoldArgs &f, const float *ibuf, long long t0, int M,
+                                           int item, int tid)
+{
+    int lo = 0, hi = f.nspans;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (f.span_b[mid] <= t0)
+            lo = mid + 1;
+        else
+            hi = mid;
+    }
+    for (int s = lo; s < f.nspans; ++s) {
+        const long long sa = f.span_a[s];
+        if (sa >= t0 + M)
+            break;
+        const int dest = f.span_dest[s];
+        if (dest != 0) {
+            const long long a = sa > t0 ? sa : t0;
+            const long long sb = f.span_b[s];
+            const long long b = sb < t0 + M ? sb : t0 + M;
+            if (a < b) {
+                const int ph_lo = f.span_phase0[s] + (int)(a - sa);
+                const int ph_hi = ph_lo + (int)(b - a);
+                const int b_lo = ph_lo / f.bpt;
+                int b_hi = (ph_hi - 1) / f.bpt;
+                if (b_hi > f.nbins - 1)
+                    b_hi = f.nbins - 1;
+                float *row = (dest == 1 ? f.part_main : f.part_pend) + (size_t)item * f.nbins;
+                const float *src = ibuf + (int)(a - t0) - ph_lo;  // src[phase]
+                for (int bin = b_lo + tid; bin <= b_hi; bin += blockDim.x) {
+                    const int s_lo = max(ph_lo, bin * f.bpt);
+                    const int s_hi = min(ph_hi, (bin + 1) * f.bpt);
+                    float sum = 0.f;
+                    for (int p = s_lo; p < s_hi; ++p)
+                        sum += src[p];
+                    row[bin] += sum;
+                }
+            }
+        }
+        __syncthreads();
+    }
+}
+
+template <int LOG2N, bool PP, bool SERIES, bool FOLD>
+__global__ void __launch_bounds__(FftShape<LOG2N>::T) dedisp_kernel(DedispArgs a)
+{
+    using F = FftShape<LOG2N>;
+    constexpr int N = F::N, M = N / 2, T = F::T;
+    constexpr int RL = F::radix(F::NST - 1);
+    extern __shared__ float2 smem[];
+    float2 *buf0 = smem;
+    float2 *buf1 = PP ? smem + F::SMEM : smem;
+    float *ibuf = reinterpret_cast<float *>(smem + (PP ? 2 : 1) * F::SMEM);
+    const int tid = threadIdx.x;
+    const int items = a.D * a.R;
+    for (int w = blockIdx.x; w < items; w += gridDim.x) {
+        const int dm = w % a.D;
+        const int rr = w / a.D;
+        const int kb = (int)((long long)a.count * rr / a.R);
+        const int ke = (int)((long long)a.count * (rr + 1) / a.R);
+        const float2 *__restrict__ Hd = a.H + (size_t)dm * N;
+        const uint16_t *__restrict__ dl = a.delays + (size_t)dm * N;
+        for (int k = kb; k < ke; ++k) {
+            const long long kg = a.k0 + k;
+            const int slot_k = (int)(kg % a.S);
+            float2 v[16];
+#pragma unroll
+            for (int r = 0; r < 16; ++r) {
+                const int b = tid + r * T;
+                const int d = (int)__ldg(&dl[b]);
+                float2 x = make_float2(0.f, 0.f);
+                if (kg >= d) {  // blocks before the stream start are zero
+                    int s = slot_k - d;
+                    if (s < 0)
+                        s += a.S;
+                    x = a.ring[(size_t)s * N + b];
+                }
+                v[r] = cmul(x, __ldg(&Hd[b]));
+            }
+            dft16<+1>(v);
+            __syncthreads();  // the previous block's readers of buf0 and ibuf are done
+            stage_store<LOG2N, 0>(v, buf0, tid);
+            run_stages<LOG2N, +1, PP>(v, buf0, buf1, tid, a.tw);
+            // keep outputs n >= M (the last-stage slots with r >= R/2)
+#pragma unroll
+            for (int slot = 0; slot < 16; ++slot) {
+                if ((slot % RL) >= RL / 2) {
+                    const int t = last_out_index<LOG2N>(tid, slot) - M;
+                    const float2 y = v[slot];
+                    if constexpr (SERIES)
+                        a.series[(size_t)dm * a.count * M + (size_t)k * M + t] = y;
+                    if constexpr (FOLD) {
+                        const float p = y.x * y.x + y.y * y.y;
+                        ibuf[t] = a.fold.detect ? sqrtf(p) : p;
+                    }
+                }
+            }
+            if constexpr (FOLD) {
+                __syncthreads();
+                fold_block(a.fold, ibuf, (long long)k * M, M, w, tid);
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// filter design on the device
+// ---------------------------------------------------------------------------
+
+// Chirp phase at offset index i with the reference's rounding sequence
+// (msosm_prepare.cpp:50-62): float w, float (w + w0), the rest in double,
+// left to right.  Explicit round-to-nearest intrinsics keep the compiler
+// from contracting any step into an FMA.
+__device__ __forceinline__ double chirp_phase(const ChirpParams &p, unsigned int i)
+{
+    const double pi = kPi;
+    const double fs = (double)p.fs;
+    const float si = __fmul_rn(p.step, __uint2float_rn(i));
+    float w = __double2float_rn(__dadd_rn(__dmul_rn(-pi, fs), (double)si));
+    w = __double2float_rn(__dadd_rn((double)w, __dmul_rn(pi, fs)));
+    const float den = __fadd_rn(w, p.w0);
+    double ph = __dmul_rn(4.0, pi);
+    ph = __dmul_rn(ph, pi);
+    ph = __dmul_rn(ph, (double)p.kdm);
+    ph = __dmul_rn(ph, (double)p.dm);
+    ph = __dmul_rn(ph, (double)w);
+    ph = __dmul_rn(ph, (double)w);
+    ph = __ddiv_rn(ph, (double)den);
+    ph = __ddiv_rn(ph, (double)p.w0);
+    ph = __ddiv_rn(ph, (double)p.w0);
+    return ph;
+}
+
+// cos/sin of a phase of up to ~1e7 rad: reduce mod 2 pi in FP64 with 2 pi
+// split into a double head and tail (Cody-Waite), then sincos.
+__device__ __forceinline__ void chirp_cis(double ph, float &c, float &s)
+{
+    constexpr double kTwoPiHi = 6.283185307179586232;     // nearest double to 2 pi
+    constexpr double kTwoPiLo = 2.4492935982947064e-16;   // 2 pi - kTwoPiHi
+    constexpr double kInvTwoPi = 0.15915494309189533577;
+    const double n = rint(ph * kInvTwoPi);
+    double r = fma(-n, kTwoPiHi, ph);
+    r = fma(-n, kTwoPiLo, r);
+    double sd, cd;
+    sincos(r, &sd, &cd);
+    c = (float)cd;
+    s = (float)sd;
+}
+
+template <int LOG2N, bool PP>
+__global__ void __launch_bounds__(FftShape<LOG2N>::T) design_kernel(DesignArgs a)
+{
+    using F = FftShape<LOG2N>;
+    using FM = FftShape<LOG2N - 1>;
+    constexpr int N = F::N, M = N / 2, T = F::T, TM = FM::T;
+    extern __shared__ float2 smem[];
+    float2 *buf0 = smem;
+    float2 *buf1 = PP ? smem + F::SMEM : smem;
+    const int tid = threadIdx.x;
+    const int dm = blockIdx.x;
+    const ChirpParams cp = a.chirp[dm];
+    const bool act = tid < TM;
+    float2 v[16];
+    if (act) {
+        // h index j holds offset index (j + M/2) mod M (msosm_prepare.cpp:50-63)
+#pragma unroll
+        for (int r = 0; r < 16; ++r) {
+            const int j = tid + r * TM;
+            const unsigned int i = (unsigned int)((j + M / 2) & (M - 1));
+            float c, s;
+            chirp_cis(chirp_phase(cp, i), c, s);
+            v[r] = make_float2(c, a.sign < 0 ? -s : s);
+        }
+        dft16<+1>(v);
+        stage_store<LOG2N - 1, 0>(v, buf0, tid);
+    }
+    run_stages<LOG2N - 1, +1, PP>(v, buf0, buf1, tid, a.tw_inv_m, act);
+    __syncthreads();
+    if (act) {
+#pragma unroll
+        for (int slot = 0; slot < 16; ++slot)
+            buf1[smem_pad(last_out_index<LOG2N - 1>(tid, slot))] = v[slot];
+    }
+    __syncthreads();
+    // zero-padded 2M-point forward transform of the M-point result
+#pragma unroll
+    for (int r = 0; r < 16; ++r) {
+        const int n = tid + r * T;
+        v[r] = n < M ? buf1[smem_pad(n)] : make_float2(0.f, 0.f);
+    }
+    __syncthreads();
+    dft16<-1>(v);
+    stage_store<LOG2N, 0>(v, buf0, tid);
+    run_stages<LOG2N, -1, PP>(v, buf0, buf1, tid, a.tw_fwd_n);
+    float2 *out = a.H + (size_t)dm * N;
+#pragma unroll
+    for (int slot = 0; slot < 16; ++slot) {
+        const float2 y = v[slot];
+        out[last_out_index<LOG2N>(tid, slot)] = make_float2(y.x * a.scale, y.y * a.scale);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// small kernels
+// ---------------------------------------------------------------------------
+
+__global__ void fold_reduce_kernel(const float *__restrict__ pm, const float *__restrict__ pp, int D, int R,
+                                   int nbins, double *am, double *ap)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= D * nbins)
+        return;
+    const int dm = i / nbins, bin = i % nbins;
+    double sm = 0.0, sp = 0.0;
+    for (int r = 0; r < R; ++r) {
+        const size_t row = ((size_t)r * D + dm) * nbins + bin;
+        sm += (double)pm[row];
+        sp += (double)pp[row];
+    }
+    am[i] += sm;
+    ap[i] += sp;
+}
+
+__global__ void fold_flush_kernel(double *am, double *ap, size_t n)
+{
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        am[i] += ap[i];
+        ap[i] = 0.0;
+    }
+}
+
+__global__ void fold_readout_kernel(const double *am, size_t n, double scale, float *out)
+{
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n)
+        out[i] = (float)(am[i] * scale);
+}
+
+// complexToUint16 (gpu/gpu_kernel.cu:317-329): uint16(v + 32768*(v != 0)),
+// truncating; out-of-range values saturate (undefined in the reference).
+__device__ __forceinline__ uint32_t encode_u16(float v)
+{
+    float u = v + (v != 0.0f ? 32768.0f : 0.0f);
+    u = fminf(fmaxf(u, 0.0f), 65535.0f);
+    return (uint32_t)u;
+}
+
+__global__ void encode_u16_kernel(const float2 *__restrict__ src, uint32_t *__restrict__ dst, size_t n)
+{
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        const float2 v = src[i];
+        dst[i] = encode_u16(v.x) | (encode_u16(v.y) << 16);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+
+bool log2n_supported(int log2n) { return log2n >= kMinLog2N && log2n <= kMaxLog2N; }
+
+template <int LOG2N>
+constexpr bool use_pingpong() { return LOG2N <= 12; }
+
+template <int LOG2N>
+size_t dedisp_smem_bytes()
+{
+    using F = FftShape<LOG2N>;
+    return (use_pingpong<LOG2N>() ? 2 : 1) * F::SMEM * sizeof(float2) + (F::N / 2) * sizeof(float);
+}
+
+template <int LOG2N>
+size_t fft_smem_bytes()
+{
+    using F = FftShape<LOG2N>;
+    return (use_pingpong<LOG2N>() ? 2 : 1) * F::SMEM * sizeof(float2);
+}
+
+template <typename K>
+static cudaError_t set_smem(K kernel, size_t bytes)
+{
+    return cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+template <int LOG2N>
+static cudaError_t forward_t(InputKind kind, const FwdArgs &a, cudaStream_t st)
+{
+    constexpr bool PP = use_pingpong<LOG2N>();
+    const size_t sm = fft_smem_bytes<LOG2N>();
+    cudaError_t e;
+    if (kind == kInputU16) {
+        auto k = forward_kernel<LOG2N, kInputU16, PP>;
+        if ((e = set_smem(k, sm)) != cudaSuccess)
+            return e;
+        k<<<a.count, FftShape<LOG2N>::T, sm, st>>>(a);
+    } else {
+        auto k = forward_kernel<LOG2N, kInputC64, PP>;
+        if ((e = set_smem(k, sm)) != cudaSuccess)
+            return e;
+        k<<<a.count, FftShape<LOG2N>::T, sm, st>>>(a);
+    }
+    return cudaGetLastError();
+}
+
+template <int LOG2N, bool SERIES, bool FOLD>
+static auto dedisp_fn() { return dedisp_kernel<LOG2N, use_pingpong<LOG2N>(), SERIES, FOLD>; }
+
+template <int LOG2N>
+static cudaError_t dedisp_t(bool series, bool fold, const DedispArgs &a, int grid, cudaStream_t st)
+{
+    const size_t sm = dedisp_smem_bytes<LOG2N>();
+    auto go = [&](auto k) -> cudaError_t {
+        cudaError_t e = set_smem(k, sm);
+        if (e != cudaSuccess)
+            return e;
+        k<<<grid, FftShape<LOG2N>::T, sm, st>>>(a);
+        return cudaGetLastError();
+    };
+    if (series && fold)
+        return go(dedisp_fn<LOG2N, true, true>());
+    if (fold)
+        return go(dedisp_fn<LOG2N, false, true>());
+    return go(dedisp_fn<LOG2N, true, false>());
+}
+
+template <int LOG2N>
+static int dedisp_occ_t(bool series, bool fold)
+{
+    const size_t sm = dedisp_smem_bytes<LOG2N>();
+    int n = 0;
+    auto occ = [&](auto k) {
+        if (set_smem(k, sm) != cudaSuccess)
+            return;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, FftShape<LOG2N>::T, sm);
+    };
+    if (series && fold)
+        occ(dedisp_fn<LOG2N, true, true>());
+    else if (fold)
+        occ(dedisp_fn<LOG2N, false, true>());
+    else
+        occ(dedisp_fn<LOG2N, true, false>());
+    return n;
+}
+
+template <int LOG2N>
+static cudaError_t design_t(const DesignArgs &a, cudaStream_t st)
+{
+    constexpr bool PP = use_pingpong<LOG2N>();
+    const size_t sm = fft_smem_bytes<LOG2N>();
+    auto k = design_kernel<LOG2N, PP>;
+    cudaError_t e = set_smem(k, sm);
+    if (e != cudaSuccess)
+        return e;
+    k<<<a.D, FftShape<LOG2N>::T, sm, st>>>(a);
+    return cudaGetLastError();
+}
+
+#define MSOSM_DISPATCH(log2n, CALL)                                                                   \
+    switch (log2n) {                                                                                  \
+    case 6: return CALL(6);                                                                           \
+    case 7: return CALL(7);                                                                           \
+    case 8: return CALL(8);                                                                           \
+    case 9: return CALL(9);                                                                           \
+    case 10: return CALL(10);                                                                         \
+    case 11: return CALL(11);                                                                         \
+    case 12: return CALL(12);                                                                         \
+    case 13: return CALL(13);                                                                         \
+    case 14: return CALL(14);                                                                         \
+    default: break;                                                                                   \
+    }
+
+cudaError_t launch_forward(int log2n, InputKind kind, const FwdArgs &a, cudaStream_t st)
+{
+#define CALL(L) forward_t<L>(kind, a, st)
+    MSOSM_DISPATCH(log2n, CALL)
+#undef CALL
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_dedisp(int log2n, bool series, bool fold, const DedispArgs &a, int grid, cudaStream_t st)
+{
+#define CALL(L) dedisp_t<L>(series, fold, a, grid, st)
+    MSOSM_DISPATCH(log2n, CALL)
+#undef CALL
+    return cudaErrorInvalidValue;
+}
+
+int dedisp_blocks_per_sm(int log2n, bool series, bool fold)
+{
+#define CALL(L) dedisp_occ_t<L>(series, fold)
+    MSOSM_DISPATCH(log2n, CALL)
+#undef CALL
+    return 0;
+}
+
+cudaError_t launch_design(int log2n, const DesignArgs &a, cudaStream_t st)
+{
+#define CALL(L) design_t<L>(a, st)
+    MSOSM_DISPATCH(log2n, CALL)
+#undef CALL
+    return cudaErrorInvalidValue;
+}
+
+static unsigned int blocks_for(size_t n, unsigned int t) { return (unsigned int)((n + t - 1) / t); }
+
+cudaError_t launch_fold_reduce(const float *pm, const float *pp, int D, int R, int nbins, double *am,
+                               double *ap, cudaStream_t st)
+{
+    const size_t n = (size_t)D * nbins;
+    fold_reduce_kernel<<<blocks_for(n, 256), 256, 0, st>>>(pm, pp, D, R, nbins, am, ap);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fold_flush(double *am, double *ap, size_t n, cudaStream_t st)
+{
+    fold_flush_kernel<<<blocks_for(n, 256), 256, 0, st>>>(am, ap, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_fold_readout(const double *am, size_t n, double scale, float *out, cudaStream_t st)
+{
+    fold_readout_kernel<<<blocks_for(n, 256), 256, 0, st>>>(am, n, scale, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_encode_u16(const float2 *src, uint32_t *dst, size_t n, cudaStream_t st)
+{
+    encode_u16_kernel<<<blocks_for(n, 256), 256, 0, st>>>(src, dst, n);
+    return cudaGetLastError();
+}
+
+}  // namespace msosm

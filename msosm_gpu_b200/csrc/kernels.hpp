@@ -1,0 +1,77 @@
+// kernels.hpp -- host-side launchers of the sm_100a kernels (kernels.cu).
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "host_prepare.hpp"
+
+namespace msosm {
+
+constexpr int kMinLog2N = 6;   // FFT 64 (M = 32) .. 16384 in one thread block
+constexpr int kMaxLog2N = 14;
+
+enum InputKind : int { kInputC64 = 0, kInputU16 = 1 };
+
+struct FwdArgs {
+    const void *input;      // count*M samples of this call (device)
+    const float2 *hist_in;  // previous call's last M samples
+    float2 *hist_out;       // this call's last M samples (for the next call)
+    float2 *ring;           // [S][N] spectra
+    int S;
+    long long k0;           // global index of this call's first block
+    int count;
+    const float2 *tw;       // exp(-2 pi i e/N)
+};
+
+struct FoldArgs {
+    const long long *span_a, *span_b;  // chunk-local [a, b), sorted
+    const int *span_phase0, *span_dest; // dest 0 skip / 1 main / 2 pending
+    int nspans;
+    int bpt;      // samples per output bin
+    int nbins;    // output bins
+    int detect;   // 0 |y|^2, 1 |y|
+    float *part_main, *part_pend;  // [items][nbins]
+};
+
+struct DedispArgs {
+    const float2 *ring;
+    int S;
+    long long k0;
+    int count;
+    int D;
+    int R;                    // block ranges per trial (work item = (range, trial))
+    const float2 *H;          // [D][N], scaled by 1/N^2
+    const uint16_t *delays;   // [D][N]
+    const float2 *tw;         // exp(+2 pi i e/N)
+    float2 *series;           // [D][count*M] or nullptr
+    FoldArgs fold;            // fold.nspans < 0: no folding
+};
+
+struct DesignArgs {
+    const ChirpParams *chirp;  // [D] device
+    int D;
+    const float2 *tw_inv_m;    // exp(+2 pi i e/M)
+    const float2 *tw_fwd_n;    // exp(-2 pi i e/N)
+    float2 *H;                 // [D][N]
+    float scale;
+    int sign;                  // -1 dedispersion (cos - i sin), +1 dispersion
+};
+
+bool log2n_supported(int log2n);
+
+cudaError_t launch_forward(int log2n, InputKind kind, const FwdArgs &a, cudaStream_t st);
+cudaError_t launch_dedisp(int log2n, bool series, bool fold, const DedispArgs &a, int grid,
+                          cudaStream_t st);
+// CTAs of the dedispersion kernel that fit on one SM (for the persistent grid)
+int dedisp_blocks_per_sm(int log2n, bool series, bool fold);
+cudaError_t launch_design(int log2n, const DesignArgs &a, cudaStream_t st);
+
+cudaError_t launch_fold_reduce(const float *part_main, const float *part_pend, int D, int R, int nbins,
+                               double *acc_main, double *acc_pend, cudaStream_t st);
+cudaError_t launch_fold_flush(double *acc_main, double *acc_pend, size_t n, cudaStream_t st);
+cudaError_t launch_fold_readout(const double *acc_main, size_t n, double scale, float *out,
+                                cudaStream_t st);
+cudaError_t launch_encode_u16(const float2 *src, uint32_t *dst, size_t n, cudaStream_t st);
+
+}  // namespace msosm
