@@ -68,8 +68,9 @@ def workload_config(samples, n_dm, ws):
 
 
 def dm_trials(rank, n_dm):
-    # weak scaling: rank r owns trials [r*100, (r+1)*100]
-    return (np.linspace(0.0, DM_MAX, n_dm) + rank * DM_MAX).astype(np.float32)
+    # weak scaling: rank r owns n_dm trials over [r*100, (r+1)*100]
+    from msosm_gpu_b200 import shard
+    return shard.weak_trials(rank, n_dm, DM_MAX)
 
 
 def make_signal(samples):
@@ -253,10 +254,8 @@ def run_ours(args):
         dist.barrier()
     ms = s.elapsed_time(e) / args.steps
     tm = d.timing()
-    t_ms = torch.tensor([ms], dtype=torch.float64, device=dev)
-    if ws > 1:
-        dist.all_reduce(t_ms, op=dist.ReduceOp.MAX)
-    ms_max = float(t_ms.item())
+    from msosm_gpu_b200 import shard
+    ms_max = shard.max_over_ranks(ms, dev)
     units = float(args.dms) * samples * ws
     value = units / (ms_max * 1e-3) / 1e6
     prof = d.get_profiles()
@@ -285,10 +284,7 @@ def run_ours(args):
         e2e_step()
     torch.cuda.synchronize()
     e2e_s = (time.perf_counter() - t0) / args.steps
-    t_e = torch.tensor([e2e_s], dtype=torch.float64, device=dev)
-    if ws > 1:
-        dist.all_reduce(t_e, op=dist.ReduceOp.MAX)
-    e2e_v = units / float(t_e.item()) / 1e6
+    e2e_v = units / shard.max_over_ranks(e2e_s, dev) / 1e6
 
     # ---- roofline of the dominant kernel (dedisp_kernel) -------------------
     log2n = int(math.log2(FFTPOINT))

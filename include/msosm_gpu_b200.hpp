@@ -1,0 +1,423 @@
+// msosm_gpu_b200.hpp -- header-only C++ drop-in for the reference's host API.
+//
+// The classes below carry the names, constructor/method signatures and
+// public fields of the reference classes in dedispersion/include/*.h
+// (msosm_gpu_batch.h, msosm_gpu_concurrent.h, msosm_gpu_batch_stream.h,
+// osm_gpu_batch.h, osm_gpu_concurrent.h, prepare*.h) and call the C ABI of
+// libmsosm_b200.so (msosm_b200.h).  A program written against the
+// reference builds against this header by swapping its includes and linking
+// -lmsosm_b200; it needs neither FFTW nor cuFFT.
+//
+// Differences a caller can observe:
+//  * errors print a message and exit(1) like the reference's CUDA_CHECK
+//    (gpu/include/gpu_common.cuh:41-61); define MSOSM_B200_THROW before the
+//    include to get std::runtime_error instead;
+//  * dedisp_params is msosm_complex* (same layout as fftwf_complex);
+//  * reset_device() and the destructors release this object's resources
+//    only (the reference calls cudaDeviceReset, which ends every allocation
+//    of the process);
+//  * get_output() waits for the copy, so the wait_for_cpu / wait_for_threads
+//    handshake of the reference (a busy-wait on a plain bool,
+//    msosm_gpu_dm_concurrent.cpp:156-160) is kept as fields but never spins;
+//  * trials with DM 0 get all block delays 0 (undefined in the reference).
+#pragma once
+
+#include <algorithm>
+#include <cstdio>
+#include <cstdlib>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "msosm_b200.h"
+
+namespace msosm_b200 {
+
+using Complex = msosm_complex;
+using uint16_pair = msosm_uint16_pair;
+
+inline void check(msosm_status s, const char *what)
+{
+    if (s == MSOSM_OK)
+        return;
+    std::string msg = std::string(what) + ": " + msosm_last_error();
+#ifdef MSOSM_B200_THROW
+    throw std::runtime_error(msg);
+#else
+    std::fprintf(stderr, "msosm error %d: %s\n", s, msg.c_str());
+    std::exit(1);
+#endif
+}
+
+// ---------------------------------------------------------------------------
+// filter design (dedispersion/include/prepare.h:7-49, :101-134)
+// ---------------------------------------------------------------------------
+
+class Prepare_MSOSM {
+public:
+    explicit Prepare_MSOSM(float bw = 0, float dm = 0, float f0 = 0) : bw_(bw), dm_(dm), f0_(f0)
+    {
+        if (bw > 0 && f0 > 0)
+            check(msosm_prepare_nd(bw, dm, f0, &Nd), "msosm_prepare_nd");
+    }
+    void calculate_min_order()
+    {
+        check(msosm_prepare_min_order_msosm(Nd, &M), "msosm_prepare_min_order_msosm");
+        M_min = M;
+    }
+    void override_order(unsigned long order) { M = order; }
+    void segmentation()
+    {
+        dp_.assign(2 * M, 0);
+        check(msosm_prepare_segmentation(bw_, dm_, f0_, M, &delaycount, dp_.data()), "segmentation");
+        delay_points = dp_.data();
+    }
+    void generate_dedisp_params()
+    {
+        H_.assign(2 * M, Complex{0.f, 0.f});
+        check(msosm_prepare_dedisp_params(bw_, dm_, f0_, M, H_.data()), "generate_dedisp_params");
+        dedisp_params = H_.data();
+    }
+
+    unsigned long M = 0, M_min = 0;
+    int delaycount = 0;
+    Complex *dedisp_params = nullptr;
+    int *delay_points = nullptr;
+    unsigned long Nd = 0;
+
+protected:
+    float bw_, dm_, f0_;
+    std::vector<int> dp_;
+    std::vector<Complex> H_;
+};
+
+namespace detail {
+
+// One msosm_dedisp handle plus the reference-shaped views of its state.
+class Handle {
+public:
+    Handle() = default;
+    Handle(const Handle &) = delete;
+    Handle &operator=(const Handle &) = delete;
+    ~Handle() { reset(); }
+    void create(const float *bw, const float *dm, const float *f0, int n, unsigned long fftpoint, int count,
+                unsigned long input_size, unsigned int flags)
+    {
+        reset();
+        check(msosm_dedisp_create(bw, dm, f0, n, fftpoint, count, input_size, flags, &h), "msosm_dedisp_create");
+        check(msosm_dedisp_get_info(h, &info), "msosm_dedisp_get_info");
+        n_ = n;
+        Nd.resize(n);
+        delaycount.resize(n);
+        check(msosm_dedisp_get_nd(h, Nd.data()), "msosm_dedisp_get_nd");
+        check(msosm_dedisp_get_delaycount(h, delaycount.data()), "msosm_dedisp_get_delaycount");
+        dp.assign((size_t)n * info.fftpoint, 0);
+        H.assign((size_t)n * info.fftpoint, Complex{0.f, 0.f});
+        for (int i = 0; i < n; ++i) {
+            check(msosm_dedisp_get_delay_points(h, i, dp.data() + (size_t)i * info.fftpoint), "delay_points");
+            check(msosm_dedisp_get_dedisp_params(h, i, H.data() + (size_t)i * info.fftpoint), "dedisp_params");
+        }
+    }
+    void reset()
+    {
+        if (h)
+            msosm_dedisp_destroy(h);
+        h = nullptr;
+    }
+    size_t block() const { return (size_t)info.count * info.M; }
+    Complex *device_output() const
+    {
+        Complex *p = nullptr;
+        check(msosm_dedisp_output_device_ptr(h, &p), "msosm_dedisp_output_device_ptr");
+        return p;
+    }
+
+    msosm_dedisp *h = nullptr;
+    msosm_dedisp_info info{};
+    int n_ = 0;
+    std::vector<unsigned long> Nd;
+    std::vector<int> delaycount;
+    std::vector<int> dp;
+    std::vector<Complex> H;
+};
+
+}  // namespace detail
+
+// ---------------------------------------------------------------------------
+// single DM (dedispersion/include/msosm_gpu_batch.h:7-41)
+// ---------------------------------------------------------------------------
+
+class MSOSM_GPU_BATCH : public Prepare_MSOSM {
+public:
+    explicit MSOSM_GPU_BATCH(float bw = 0, float dm = 0, float f0 = 0) : Prepare_MSOSM(bw, dm, f0) {}
+    void get_device_info() { std::printf("CUDA devices: %d\n", msosm_device_count()); }
+    void initialize_uint16(unsigned long fftpoint = 0, int count = 1)
+    {
+        h_.create(&bw_, &dm_, &f0_, 1, fftpoint, count, 0, 0);
+        M = h_.info.M;
+        M_min = h_.info.M_min;
+        this->count = h_.info.count;
+        delaycount = h_.delaycount[0];
+        delay_points = h_.dp.data();
+        dedisp_params = h_.H.data();
+        output_buffer_d = h_.device_output();
+    }
+    void filter_block_uint16(uint16_pair *input)
+    {
+        check(msosm_dedisp_filter_block_uint16(h_.h, input), "filter_block_uint16");
+    }
+    void get_output(Complex *output)
+    {
+        // the handle's buffer ends with one extra element; copy count*M
+        out_.resize(h_.block() + 1);
+        check(msosm_dedisp_get_output_c64(h_.h, out_.data()), "get_output");
+        std::copy(out_.begin(), out_.end() - 1, output);
+    }
+
+    int count = 0;
+    Complex *output_buffer_d = nullptr;
+
+protected:
+    detail::Handle h_;
+    std::vector<Complex> out_;
+};
+
+// classical overlap-save (dedispersion/include/osm_gpu_batch.h:7-37)
+class OSM_GPU_BATCH : public MSOSM_GPU_BATCH {
+public:
+    explicit OSM_GPU_BATCH(float bw = 0, float dm = 0, float f0 = 0) : MSOSM_GPU_BATCH(bw, dm, f0) {}
+    void initialize_uint16(unsigned long fftpoint = 0, int count = 1, bool streaming = false)
+    {
+        (void)streaming;
+        h_.create(&bw_, &dm_, &f0_, 1, fftpoint, count, 0, MSOSM_FLAG_OSM);
+        M = h_.info.M;
+        M_min = h_.info.M_min;
+        this->count = h_.info.count;
+        dedisp_params = h_.H.data();
+        output_buffer_d = h_.device_output();
+        total_memory = h_.info.device_bytes;
+    }
+    unsigned long total_memory = 0;
+};
+
+// ---------------------------------------------------------------------------
+// many DMs over one input (dedispersion/include/msosm_gpu_concurrent.h:15-64)
+// ---------------------------------------------------------------------------
+
+class MSOSM_GPU_DM_concurrent {
+public:
+    MSOSM_GPU_DM_concurrent(float *bw, float *dm, float *f0, int numDMs)
+        : numDMs(numDMs), bw_(bw, bw + numDMs), dm_(dm, dm + numDMs), f0_(f0, f0 + numDMs)
+    {
+    }
+    virtual ~MSOSM_GPU_DM_concurrent() = default;
+    void get_device_info() { std::printf("CUDA devices: %d\n", msosm_device_count()); }
+    void initialize_uint16(unsigned long fftpoint, int count = 1, unsigned long input_size = 0,
+                           bool compute_only = false)
+    {
+        create(fftpoint, count, input_size, 0);
+        this->compute_only = compute_only;
+    }
+    void initialize_threads_flag(int thread_num) { wait_for_threads.assign(thread_num, false); }
+    void filter_block_uint16(uint16_pair *input)
+    {
+        check(msosm_dedisp_filter_block_uint16(h_.h, input), "filter_block_uint16");
+    }
+    // numDMs*count*M + 1 elements, [dm][count*M] then a trailing zero
+    void get_output(Complex *output) { check(msosm_dedisp_get_output_c64(h_.h, output), "get_output"); }
+    void get_output(uint16_pair *output)
+    {
+        check(msosm_dedisp_get_output_uint16(h_.h, output), "get_output");
+    }
+    void get_output_thread(uint16_pair *output, int thread_id)
+    {
+        (void)thread_id;
+        get_output(output);
+    }
+    void synchronize() { check(msosm_dedisp_synchronize(h_.h), "synchronize"); }
+    void reset_device() { h_.reset(); }
+
+    int count = 0;
+    bool wait_for_cpu = false;
+    std::vector<bool> wait_for_threads;
+    unsigned long M_common = 0, M_common_min = 0;
+    std::vector<unsigned long> Nd;
+    std::vector<int> delaycount;
+    int numDMs;
+    // per-trial views (Prepare_MSOSM_DM_concurrent::delay_points / dedisp_params)
+    int *delay_points_of(int i) { return h_.dp.data() + (size_t)i * h_.info.fftpoint; }
+    Complex *dedisp_params_of(int i) { return h_.H.data() + (size_t)i * h_.info.fftpoint; }
+
+protected:
+    void create(unsigned long fftpoint, int count, unsigned long input_size, unsigned int flags)
+    {
+        h_.create(bw_.data(), dm_.data(), f0_.data(), numDMs, fftpoint, count, input_size, flags);
+        this->count = h_.info.count;
+        M_common = h_.info.M;
+        M_common_min = h_.info.M_min;
+        Nd = h_.Nd;
+        delaycount = h_.delaycount;
+    }
+    bool compute_only = false;
+    std::vector<float> bw_, dm_, f0_;
+    detail::Handle h_;
+};
+
+// dedispersion/include/osm_gpu_concurrent.h:7-42
+class OSM_GPU_DM_concurrent : public MSOSM_GPU_DM_concurrent {
+public:
+    using MSOSM_GPU_DM_concurrent::MSOSM_GPU_DM_concurrent;
+    void initialize_uint16(unsigned long fftpoint = 0, int count = 1, bool compute_only = false)
+    {
+        create(fftpoint, count, 0, MSOSM_FLAG_OSM);
+        this->compute_only = compute_only;
+    }
+};
+
+// ---------------------------------------------------------------------------
+// one DM per output, one input, processed DM by DM
+// (dedispersion/include/msosm_gpu_batch.h:43-77)
+// ---------------------------------------------------------------------------
+
+class MSOSM_GPU_DM_BATCH_loop {
+public:
+    MSOSM_GPU_DM_BATCH_loop(float *bw, float *dm, float *f0, int numOutput)
+        : numOutput(numOutput), bw_(bw, bw + numOutput), dm_(dm, dm + numOutput), f0_(f0, f0 + numOutput)
+    {
+    }
+    void get_device_info() { std::printf("CUDA devices: %d\n", msosm_device_count()); }
+    void initialize_uint16(unsigned long fftpoint, int count = 1)
+    {
+        h_.create(bw_.data(), dm_.data(), f0_.data(), numOutput, fftpoint, count, 0, 0);
+        this->count = h_.info.count;
+        M_loop = h_.info.M;
+        M_loop_min = h_.info.M_min;
+        Nd = h_.Nd;
+        delaycount = h_.delaycount;
+    }
+    // every trial is dedispersed here; filter_block_uint16(out, i) then
+    // copies trial i (the reference runs trial i's filter at that point)
+    void input_process(uint16_pair *input)
+    {
+        check(msosm_dedisp_filter_block_uint16(h_.h, input), "input_process");
+        all_.resize((size_t)numOutput * h_.block() + 1);
+        check(msosm_dedisp_get_output_c64(h_.h, all_.data()), "get_output");
+    }
+    void filter_block_uint16(Complex **output, int i)
+    {
+        std::copy(all_.begin() + (size_t)i * h_.block(), all_.begin() + (size_t)(i + 1) * h_.block(), output[i]);
+    }
+    void synchronize() { check(msosm_dedisp_synchronize(h_.h), "synchronize"); }
+
+    int count = 0;
+    int numOutput;
+    unsigned long M_loop = 0, M_loop_min = 0;
+    std::vector<unsigned long> Nd;
+    std::vector<int> delaycount;
+
+private:
+    std::vector<float> bw_, dm_, f0_;
+    detail::Handle h_;
+    std::vector<Complex> all_;
+};
+
+// one DM per stream over one input (dedispersion/include/msosm_gpu_batch_stream.h:52-93)
+class MSOSM_GPU_DM_BATCH_stream : public MSOSM_GPU_DM_concurrent {
+public:
+    MSOSM_GPU_DM_BATCH_stream(float *bw, float *dm, float *f0, int numStreams)
+        : MSOSM_GPU_DM_concurrent(bw, dm, f0, numStreams), numStreams(numStreams)
+    {
+    }
+    void initialize_uint16(unsigned long fftpoint, int count = 1)
+    {
+        create(fftpoint, count, 0, 0);
+        M_stream = M_common;
+        M_stream_min = M_common_min;
+    }
+    void get_output(Complex **output)
+    {
+        all_.resize((size_t)numStreams * block() + 1);
+        check(msosm_dedisp_get_output_c64(h_.h, all_.data()), "get_output");
+        for (int i = 0; i < numStreams; ++i)
+            std::copy(all_.begin() + (size_t)i * block(), all_.begin() + (size_t)(i + 1) * block(), output[i]);
+    }
+    void get_output(uint16_pair **output)
+    {
+        u_.resize((size_t)numStreams * block() + 1);
+        check(msosm_dedisp_get_output_uint16(h_.h, u_.data()), "get_output");
+        for (int i = 0; i < numStreams; ++i)
+            std::copy(u_.begin() + (size_t)i * block(), u_.begin() + (size_t)(i + 1) * block(), output[i]);
+    }
+    int numStreams;
+    unsigned long M_stream = 0, M_stream_min = 0;
+
+private:
+    size_t block() const { return (size_t)count * M_common; }
+    std::vector<Complex> all_;
+    std::vector<uint16_pair> u_;
+};
+
+// ---------------------------------------------------------------------------
+// independent single-DM pipelines, one input each
+// (dedispersion/include/msosm_gpu_batch_stream.h:14-49)
+// ---------------------------------------------------------------------------
+
+class MSOSM_GPU_BATCH_stream {
+public:
+    MSOSM_GPU_BATCH_stream(float *bw, float *dm, float *f0, int numStreams)
+        : numStreams(numStreams), bw_(bw, bw + numStreams), dm_(dm, dm + numStreams), f0_(f0, f0 + numStreams),
+          h_(numStreams)
+    {
+    }
+    void get_device_info() { std::printf("CUDA devices: %d\n", msosm_device_count()); }
+    // fftpoint[i] per stream (raised to the minimum and written back, as the reference does)
+    void initialize_uint16(unsigned long *fftpoint, int count = 1)
+    {
+        M.resize(numStreams);
+        M_min.resize(numStreams);
+        Nd.resize(numStreams);
+        delaycount.resize(numStreams);
+        output_buffer_d.resize(numStreams);
+        for (int i = 0; i < numStreams; ++i) {
+            h_[i].create(&bw_[i], &dm_[i], &f0_[i], 1, fftpoint[i], count, 0, 0);
+            M[i] = h_[i].info.M;
+            M_min[i] = h_[i].info.M_min;
+            fftpoint[i] = h_[i].info.fftpoint;
+            Nd[i] = h_[i].Nd[0];
+            delaycount[i] = h_[i].delaycount[0];
+            output_buffer_d[i] = h_[i].device_output();
+        }
+        this->count = count;
+    }
+    void filter_block_uint16(uint16_pair **input)
+    {
+        for (int i = 0; i < numStreams; ++i)
+            check(msosm_dedisp_filter_block_uint16(h_[i].h, input[i]), "filter_block_uint16");
+    }
+    void get_output(Complex **output)
+    {
+        for (int i = 0; i < numStreams; ++i) {
+            out_.resize(h_[i].block() + 1);
+            check(msosm_dedisp_get_output_c64(h_[i].h, out_.data()), "get_output");
+            std::copy(out_.begin(), out_.end() - 1, output[i]);
+        }
+    }
+    void synchronize()
+    {
+        for (auto &h : h_)
+            check(msosm_dedisp_synchronize(h.h), "synchronize");
+    }
+
+    int count = 0;
+    int numStreams;
+    std::vector<unsigned long> M, M_min, Nd;
+    std::vector<int> delaycount;
+    std::vector<Complex *> output_buffer_d;
+
+private:
+    std::vector<float> bw_, dm_, f0_;
+    std::vector<detail::Handle> h_;
+    std::vector<Complex> out_;
+};
+
+}  // namespace msosm_b200

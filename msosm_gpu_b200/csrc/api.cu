@@ -4,6 +4,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <new>
 #include <string>
@@ -94,6 +95,7 @@ struct msosm_dedisp {
     unsigned long M = 0, N = 0, M_min = 0;
     unsigned int flags = 0;
     bool series = true;
+    bool pingpong = false;  // tuning: MSOSM_DEDISP_PINGPONG=1 selects the two-buffer kernel
     std::vector<unsigned long> Nd;
     std::vector<int> dc;
     std::vector<int> delays;  // D x N (host copy)
@@ -111,7 +113,7 @@ struct msosm_dedisp {
     uint32_t *u16_out = nullptr;
     // folding
     bool fold = false;
-    int detect = 0, nbins = 0, bpt = 1, span_cap = 0;
+    int detect = 0, nbins = 0, bpt = 1, span_cap = 0, win_cap = 64;
     unsigned long ps = 0;
     double out_scale = 1.0;
     FoldPlanner *planner = nullptr;
@@ -203,6 +205,33 @@ msosm_status design_filters(int log2n, const std::vector<ChirpParams> &cp, float
     if (e != cudaSuccess)
         return cuda_fail(e, "filter design");
     return MSOSM_OK;
+}
+
+// Persistent grid of the dedispersion kernel: work items (block range,
+// trial), about eight per resident CTA, spread evenly over the waves.
+cudaError_t plan_grid(msosm_dedisp *d)
+{
+    int dev = 0, sms = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess)
+        e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (e != cudaSuccess)
+        return e;
+    const size_t extra = d->fold ? fold_smem_bytes(d->nbins, d->win_cap, d->nbins <= kMaxSmemBins) : 0;
+    int per_sm = dedisp_blocks_per_sm(d->log2n, d->pingpong, d->series, d->fold, extra);
+    if (per_sm < 1)
+        per_sm = 1;
+    const long long resident = (long long)per_sm * sms;
+    long long R = (8 * resident + d->D - 1) / d->D;
+    if (R > d->count)
+        R = d->count;
+    if (R < 1)
+        R = 1;
+    d->R = (int)R;
+    const long long items = (long long)d->D * R;
+    const long long waves = (items + resident - 1) / resident;
+    d->grid = (int)((items + waves - 1) / waves);
+    return cudaSuccess;
 }
 
 msosm_status check_handle(const msosm_dedisp *d)
@@ -378,8 +407,20 @@ msosm_status msosm_dedisp_create(const float *bw, const float *dm, const float *
         release(d);
         return fail(MSOSM_ERR_NO_DEVICE, "no CUDA device");
     }
-    // spectra of blocks [k0 - max_delay, k0 + count) must be resident
-    d->S = count + d->max_delay;
+    // spectra of blocks [k0 - max_delay, k0 + count) must be resident; a
+    // power-of-two depth turns the slot arithmetic into a mask
+    {
+        long long need = (long long)count + d->max_delay, S = 1;
+        while (S < need)
+            S <<= 1;
+        if (S > (1ll << 30)) {
+            release(d);
+            return fail(MSOSM_ERR_BAD_ARG, "count + max delay too large");
+        }
+        d->S = (int)S;
+    }
+    if (const char *pp = std::getenv("MSOSM_DEDISP_PINGPONG"))
+        d->pingpong = std::atoi(pp) != 0;
 
 #define CKD(call)                                                                                      \
     do {                                                                                               \
@@ -431,23 +472,7 @@ msosm_status msosm_dedisp_create(const float *bw, const float *dm, const float *
         release(d);
         return s;
     }
-    // persistent grid: work items (block range, trial), balanced over waves
-    int dev = 0, sms = 0;
-    CKD(cudaGetDevice(&dev));
-    CKD(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    int per_sm = dedisp_blocks_per_sm(log2n, d->series, false);
-    if (per_sm < 1)
-        per_sm = 1;
-    const long long resident = (long long)per_sm * sms;
-    long long R = (8 * resident + numDMs - 1) / numDMs;
-    if (R > count)
-        R = count;
-    if (R < 1)
-        R = 1;
-    d->R = (int)R;
-    const long long items = (long long)numDMs * R;
-    const long long waves = (items + resident - 1) / resident;
-    d->grid = (int)((items + waves - 1) / waves);
+    CKD(plan_grid(d));
 #undef CKD
     *out = d;
     return MSOSM_OK;
@@ -579,6 +604,7 @@ static msosm_status filter_block(msosm_dedisp *d, const void *input, InputKind k
     DedispArgs da;
     da.ring = d->ring;
     da.S = d->S;
+    da.max_delay = d->max_delay;
     da.k0 = fa.k0;
     da.count = d->count;
     da.D = d->D;
@@ -627,12 +653,14 @@ static msosm_status filter_block(msosm_dedisp *d, const void *input, InputKind k
         da.fold.detect = d->detect;
         da.fold.part_main = d->part_main;
         da.fold.part_pend = d->part_pend;
+        da.fold.smem_prof = d->nbins <= kMaxSmemBins ? 1 : 0;
+        da.fold.span_cap = d->win_cap;
     }
     // the partial-row clears and the flush above belong to the fold time;
     // the dedispersion kernel is timed alone
     if (ev)
         CK(cudaEventRecord(ev->e[2], d->stream));
-    CK(launch_dedisp(d->log2n, d->series, d->fold, da, d->grid, d->stream));
+    CK(launch_dedisp(d->log2n, d->pingpong, d->series, d->fold, da, d->grid, d->stream));
     d->launches += 1;
     if (ev)
         CK(cudaEventRecord(ev->e[3], d->stream));
@@ -727,6 +755,19 @@ msosm_status msosm_dedisp_fold_init(msosm_dedisp *d, float period, float fs, uns
     d->out_scale = nb == ps ? 1.0 : 1.0 / (double)d->bpt;
     d->detect = detect;
     d->span_cap = (int)((unsigned long)d->count * d->M / ps) + 8;
+    // spans one block can touch: ceil(M/ps) + 2 periods
+    d->win_cap = (int)(d->M / ps) + 4;
+    if (d->win_cap < 64)
+        d->win_cap = 64;
+    d->fold = true;
+    {
+        cudaError_t e = plan_grid(d);
+        if (e != cudaSuccess) {
+            d->fold = false;
+            return cuda_fail(e, "plan_grid");
+        }
+    }
+    d->fold = false;
     size_t &tot = d->device_bytes;
     const size_t prow = (size_t)d->D * d->R * d->nbins;
     const size_t nacc = (size_t)d->D * d->nbins;

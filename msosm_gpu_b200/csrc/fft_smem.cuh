@@ -167,18 +167,55 @@ struct FftShape {
     static constexpr int SMEM = smem_elems(N);  // float2 elements per buffer
 };
 
-// Load of stage S from shared memory.
+// Shared-memory addressing.  For stages S >= 1 the load stride N/R and, for
+// stores, the sub-transform size NS are multiples of 16, so
+// smem_pad(base + r*X) = smem_pad(base) + r*(X + X/16): one padded base per
+// butterfly and compile-time offsets per element.  Stage 0 (NS = 1) stores
+// element r of butterfly j at 16j + r, padded 17j + r.
+
+// Load of stage S (S >= 1) from shared memory.
 template <int LOG2N, int S>
 __device__ __forceinline__ void stage_load(float2 (&v)[16], const float2 *__restrict__ buf, int tid)
 {
     using F = FftShape<LOG2N>;
     constexpr int R = F::radix(S), B = 16 / R, STRIDE = F::N / R;
+    static_assert(S >= 1 && STRIDE % 16 == 0, "stride must be a multiple of 16");
+    constexpr int PSTRIDE = STRIDE + STRIDE / 16;
 #pragma unroll
     for (int q = 0; q < B; ++q) {
         const int j = tid + q * F::T;
+        const float2 *p = buf + smem_pad(j);
 #pragma unroll
         for (int r = 0; r < R; ++r)
-            v[q * R + r] = buf[smem_pad(j + r * STRIDE)];
+            v[q * R + r] = p[r * PSTRIDE];
+    }
+}
+
+// Twiddles W^(sign*m*r), r = 1..R-1, from two table reads (W^m and W^(4m))
+// and at most three complex products each, tw[e] = exp(sign 2 pi i e / N).
+template <int R>
+__device__ __forceinline__ void twiddle_powers(float2 (&w)[16], const float2 *__restrict__ tw, int idx1, int idx4)
+{
+    w[1] = __ldg(&tw[idx1]);
+    if constexpr (R > 2) {
+        w[2] = cmul(w[1], w[1]);
+        w[3] = cmul(w[2], w[1]);
+    }
+    if constexpr (R > 4) {
+        w[4] = __ldg(&tw[idx4]);
+        w[5] = cmul(w[4], w[1]);
+        w[6] = cmul(w[4], w[2]);
+        w[7] = cmul(w[4], w[3]);
+    }
+    if constexpr (R > 8) {
+        w[8] = cmul(w[4], w[4]);
+        w[9] = cmul(w[8], w[1]);
+        w[10] = cmul(w[8], w[2]);
+        w[11] = cmul(w[8], w[3]);
+        w[12] = cmul(w[8], w[4]);
+        w[13] = cmul(w[12], w[1]);
+        w[14] = cmul(w[12], w[2]);
+        w[15] = cmul(w[12], w[3]);
     }
 }
 
@@ -194,9 +231,11 @@ __device__ __forceinline__ void stage_compute(float2 (&v)[16], int tid, const fl
             const int j = tid + q * F::T;
             const int m = j & (NS - 1);
             constexpr int STEP = F::N / (NS * R);
+            float2 w[16];
+            twiddle_powers<R>(w, tw, m * STEP, 4 * m * STEP);
 #pragma unroll
             for (int r = 1; r < R; ++r)
-                v[q * R + r] = cmul(v[q * R + r], __ldg(&tw[m * r * STEP]));
+                v[q * R + r] = cmul(v[q * R + r], w[r]);
         }
         dft<R, SIGN>(&v[q * R]);
     }
@@ -210,10 +249,19 @@ __device__ __forceinline__ void stage_store(const float2 (&v)[16], float2 *__res
 #pragma unroll
     for (int q = 0; q < B; ++q) {
         const int j = tid + q * F::T;
-        const int base = (j / NS) * NS * R + (j & (NS - 1));
+        if constexpr (NS == 1) {
+            float2 *p = buf + 17 * j;
 #pragma unroll
-        for (int r = 0; r < R; ++r)
-            buf[smem_pad(base + r * NS)] = v[q * R + r];
+            for (int r = 0; r < R; ++r)
+                p[r] = v[q * R + r];
+        } else {
+            static_assert(NS % 16 == 0, "sub-transform size must be a multiple of 16");
+            constexpr int PNS = NS + NS / 16;
+            float2 *p = buf + smem_pad((j / NS) * NS * R + (j & (NS - 1)));
+#pragma unroll
+            for (int r = 0; r < R; ++r)
+                p[r * PNS] = v[q * R + r];
+        }
     }
 }
 

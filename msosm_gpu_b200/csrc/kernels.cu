@@ -75,7 +75,7 @@ __global__ void __launch_bounds__(FftShape<LOG2N>::T) forward_kernel(FwdArgs a)
     dft16<-1>(v);
     stage_store<LOG2N, 0>(v, buf0, tid);
     run_stages<LOG2N, -1, PP>(v, buf0, buf1, tid, a.tw);
-    float2 *row = a.ring + (size_t)((a.k0 + c) % a.S) * N;
+    float2 *row = a.ring + (size_t)((a.k0 + c) & (a.S - 1)) * N;
 #pragma unroll
     for (int slot = 0; slot < 16; ++slot)
         row[last_out_index<LOG2N>(tid, slot)] = v[slot];
@@ -85,52 +85,130 @@ __global__ void __launch_bounds__(FftShape<LOG2N>::T) forward_kernel(FwdArgs a)
 // fused dedispersion + detection + folding
 // ---------------------------------------------------------------------------
 
-// Fold the M intensities of one block (ibuf, chunk-local samples t0 ..
-// t0+M-1) into the work item's partial-profile rows.  Spans come from the
-// host fold planner (sorted, disjoint).  Every bin of one span is summed by
-// one thread in sample order; spans are separated by barriers, so a bin is
-// never updated by two threads at once and the result does not depend on
-// scheduling.
-__device__ __forceinline__ void fold_block(const FoldArgs &f, const float *ibuf, long long t0, int M,
-                                           int item, int tid)
+// Folding inside the dedispersion kernel.  The host fold planner cuts each
+// call's output samples into spans (one period each, sorted); a work item
+// keeps a window of them in shared memory and its two partial profiles
+// (complete periods, pending period) in shared memory too.  Every bin of a
+// span piece is summed by one warp (lanes strided over its samples, then a
+// fixed xor-butterfly) or, for bins of fewer than 16 samples, by one thread
+// in sample order; span pieces are separated by barriers.  The result does
+// not depend on scheduling.
+struct FoldSmem {
+    float *prof_main, *prof_pend;  // [nbins] each (or the global rows)
+    long long *wa, *wb;            // span window
+    int *wp, *wd;
+};
+
+__device__ __forceinline__ int span_lower_bound(const long long *b, int n, long long t)
 {
-    int lo = 0, hi = f.nspans;
+    int lo = 0, hi = n;
     while (lo < hi) {
         const int mid = (lo + hi) >> 1;
-        if (f.span_b[mid] <= t0)
+        if (b[mid] <= t)
             lo = mid + 1;
         else
             hi = mid;
     }
-    for (int s = lo; s < f.nspans; ++s) {
-        const long long sa = f.span_a[s];
+    return lo;
+}
+
+// Load spans [at, at + cap) into the window (all threads; barriers inside).
+__device__ __forceinline__ void span_refill(const FoldArgs &f, FoldSmem &w, int at, int &base, int &cnt)
+{
+    __syncthreads();
+    const int n = min(f.span_cap, f.nspans - at);
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        w.wa[i] = f.span_a[at + i];
+        w.wb[i] = f.span_b[at + i];
+        w.wp[i] = f.span_phase0[at + i];
+        w.wd[i] = f.span_dest[at + i];
+    }
+    base = at;
+    cnt = n;
+    __syncthreads();
+}
+
+// ibuf holds intensities at index t + t/32 (one pad slot per 32 samples), so
+// that threads reading bins of any length hit different banks
+__device__ __forceinline__ int ipad(int t) { return t + (t >> 5); }
+
+__device__ __forceinline__ void fold_piece(const FoldArgs &f, float *prof, const float *ibuf, int off,
+                                           int ph_lo, int ph_hi)
+{
+    // sample of phase p sits at chunk-local block offset off + p.  Each bin is
+    // summed by a group of G lanes (G ~ bpt/8, a power of two <= 32), lane l
+    // taking samples l, l+G, ...; the group then reduces with a fixed xor
+    // butterfly.  G*bins ~ M/8 keeps every warp of the block busy for any bin
+    // length, and the loop trip count is uniform so whole warps shuffle.
+    const int b_lo = ph_lo / f.bpt;
+    int b_hi = (ph_hi - 1) / f.bpt;
+    if (b_hi > f.nbins - 1)
+        b_hi = f.nbins - 1;
+    if (b_hi < b_lo)
+        return;
+    int G = 1;
+    while (G < 32 && G * 8 < f.bpt)
+        G <<= 1;
+    if ((int)blockDim.x < 32)
+        G = 1;  // tiny FFTs: blocks of fewer than 32 threads
+    const int g = threadIdx.x / G, l = threadIdx.x % G, ngroups = blockDim.x / G;
+    for (int first = b_lo; first <= b_hi; first += ngroups) {
+        const int bin = first + g;
+        float a0 = 0.f, a1 = 0.f;
+        if (bin <= b_hi) {
+            const int s_lo = max(ph_lo, bin * f.bpt);
+            const int s_hi = min(ph_hi, (bin + 1) * f.bpt);
+            int p = s_lo + l;
+            for (; p + G < s_hi; p += 2 * G) {
+                a0 += ibuf[ipad(off + p)];
+                a1 += ibuf[ipad(off + p + G)];
+            }
+            if (p < s_hi)
+                a0 += ibuf[ipad(off + p)];
+        }
+        float sum = a0 + a1;
+        for (int o = G >> 1; o > 0; o >>= 1)
+            sum += __shfl_xor_sync(0xffffffffu, sum, o);
+        if (bin <= b_hi && l == 0)
+            prof[bin] += sum;
+    }
+}
+
+// Fold the M intensities of one block (ibuf: chunk-local samples t0..t0+M-1).
+// sp/base/cnt: the work item's running span cursor and window (uniform).
+__device__ __forceinline__ void fold_block(const FoldArgs &f, FoldSmem &w, const float *ibuf, long long t0, int M,
+                                           int &sp, int &base, int &cnt)
+{
+    // advance to the first span ending after t0
+    while (sp < f.nspans) {
+        if (sp < base || sp >= base + cnt)
+            span_refill(f, w, sp, base, cnt);
+        if (w.wb[sp - base] <= t0)
+            ++sp;
+        else
+            break;
+    }
+    for (int s = sp; s < f.nspans; ++s) {
+        if (s >= base + cnt)
+            span_refill(f, w, s, base, cnt);
+        const int i = s - base;
+        const long long sa = w.wa[i];
         if (sa >= t0 + M)
             break;
-        const int dest = f.span_dest[s];
+        const int dest = w.wd[i];
         if (dest != 0) {
             const long long a = sa > t0 ? sa : t0;
-            const long long sb = f.span_b[s];
+            const long long sb = w.wb[i];
             const long long b = sb < t0 + M ? sb : t0 + M;
             if (a < b) {
-                const int ph_lo = f.span_phase0[s] + (int)(a - sa);
+                const int ph_lo = w.wp[i] + (int)(a - sa);
                 const int ph_hi = ph_lo + (int)(b - a);
-                const int b_lo = ph_lo / f.bpt;
-                int b_hi = (ph_hi - 1) / f.bpt;
-                if (b_hi > f.nbins - 1)
-                    b_hi = f.nbins - 1;
-                float *row = (dest == 1 ? f.part_main : f.part_pend) + (size_t)item * f.nbins;
-                const float *src = ibuf + (int)(a - t0) - ph_lo;  // src[phase]
-                for (int bin = b_lo + tid; bin <= b_hi; bin += blockDim.x) {
-                    const int s_lo = max(ph_lo, bin * f.bpt);
-                    const int s_hi = min(ph_hi, (bin + 1) * f.bpt);
-                    float sum = 0.f;
-                    for (int p = s_lo; p < s_hi; ++p)
-                        sum += src[p];
-                    row[bin] += sum;
-                }
+                fold_piece(f, dest == 1 ? w.prof_main : w.prof_pend, ibuf, (int)(a - t0) - ph_lo, ph_lo, ph_hi);
             }
+            // a later span of this block may fold into the same bins
+            if (w.wb[i] < t0 + M)
+                __syncthreads();
         }
-        __syncthreads();
     }
 }
 
@@ -144,6 +222,17 @@ __global__ void __launch_bounds__(FftShape<LOG2N>::T) dedisp_kernel(DedispArgs a
     float2 *buf0 = smem;
     float2 *buf1 = PP ? smem + F::SMEM : smem;
     float *ibuf = reinterpret_cast<float *>(smem + (PP ? 2 : 1) * F::SMEM);
+    FoldSmem fw;
+    if constexpr (FOLD) {
+        // after ibuf: [span window a, b (8-byte)] [phase0, dest] [prof_main, prof_pend]
+        long long *sp8 = reinterpret_cast<long long *>(ibuf + ibuf_floats(M));
+        fw.wa = sp8;
+        fw.wb = sp8 + a.fold.span_cap;
+        fw.wp = reinterpret_cast<int *>(sp8 + 2 * a.fold.span_cap);
+        fw.wd = fw.wp + a.fold.span_cap;
+        fw.prof_main = reinterpret_cast<float *>(fw.wd + a.fold.span_cap);
+        fw.prof_pend = fw.prof_main + a.fold.nbins;
+    }
     const int tid = threadIdx.x;
     const int items = a.D * a.R;
     for (int w = blockIdx.x; w < items; w += gridDim.x) {
@@ -153,25 +242,47 @@ __global__ void __launch_bounds__(FftShape<LOG2N>::T) dedisp_kernel(DedispArgs a
         const int ke = (int)((long long)a.count * (rr + 1) / a.R);
         const float2 *__restrict__ Hd = a.H + (size_t)dm * N;
         const uint16_t *__restrict__ dl = a.delays + (size_t)dm * N;
-        for (int k = kb; k < ke; ++k) {
-            const long long kg = a.k0 + k;
-            const int slot_k = (int)(kg % a.S);
+        int sp = 0, sbase = 0, scnt = 0;
+        if constexpr (FOLD) {
+            if (a.fold.smem_prof) {
+                for (int i = tid; i < 2 * a.fold.nbins; i += blockDim.x)
+                    fw.prof_main[i] = 0.f;
+            } else {
+                fw.prof_main = a.fold.part_main + (size_t)w * a.fold.nbins;
+                fw.prof_pend = a.fold.part_pend + (size_t)w * a.fold.nbins;
+            }
+            sp = span_lower_bound(a.fold.span_b, a.fold.nspans, (long long)kb * M);
+            span_refill(a.fold, fw, sp, sbase, scnt);
+        }
+        long long kg = a.k0 + kb;
+        const int smask = a.S - 1;  // the ring depth is a power of two
+        for (int k = kb; k < ke; ++k, ++kg) {
             float2 v[16];
+            const int slot_k = (int)(kg & smask);
+            if (kg >= a.max_delay) {
 #pragma unroll
-            for (int r = 0; r < 16; ++r) {
-                const int b = tid + r * T;
-                const int d = (int)__ldg(&dl[b]);
-                float2 x = make_float2(0.f, 0.f);
-                if (kg >= d) {  // blocks before the stream start are zero
-                    int s = slot_k - d;
-                    if (s < 0)
-                        s += a.S;
-                    x = a.ring[(size_t)s * N + b];
+                for (int r = 0; r < 16; ++r) {
+                    const int b = tid + r * T;
+                    const int s = (slot_k - (int)__ldg(&dl[b])) & smask;
+                    v[r] = cmul(a.ring[(size_t)s * N + b], __ldg(&Hd[b]));
                 }
-                v[r] = cmul(x, __ldg(&Hd[b]));
+            } else {
+#pragma unroll
+                for (int r = 0; r < 16; ++r) {
+                    const int b = tid + r * T;
+                    const int d = (int)__ldg(&dl[b]);
+                    float2 x = make_float2(0.f, 0.f);
+                    if (kg >= d)  // blocks before the stream start are zero
+                        x = a.ring[(size_t)((slot_k - d) & smask) * N + b];
+                    v[r] = cmul(x, __ldg(&Hd[b]));
+                }
             }
             dft16<+1>(v);
-            __syncthreads();  // the previous block's readers of buf0 and ibuf are done
+            // the previous block's last-stage loads (and fold reads of ibuf)
+            // must be done before buf0 is overwritten; with folding the
+            // barrier ahead of the fold already separates them
+            if constexpr (!FOLD)
+                __syncthreads();
             stage_store<LOG2N, 0>(v, buf0, tid);
             run_stages<LOG2N, +1, PP>(v, buf0, buf1, tid, a.tw);
             // keep outputs n >= M (the last-stage slots with r >= R/2)
@@ -184,14 +295,26 @@ __global__ void __launch_bounds__(FftShape<LOG2N>::T) dedisp_kernel(DedispArgs a
                         a.series[(size_t)dm * a.count * M + (size_t)k * M + t] = y;
                     if constexpr (FOLD) {
                         const float p = y.x * y.x + y.y * y.y;
-                        ibuf[t] = a.fold.detect ? sqrtf(p) : p;
+                        ibuf[ipad(t)] = a.fold.detect ? sqrtf(p) : p;
                     }
                 }
             }
             if constexpr (FOLD) {
                 __syncthreads();
-                fold_block(a.fold, ibuf, (long long)k * M, M, w, tid);
+                fold_block(a.fold, fw, ibuf, (long long)k * M, M, sp, sbase, scnt);
             }
+        }
+        if constexpr (FOLD) {
+            __syncthreads();
+            if (a.fold.smem_prof) {
+                float *gm = a.fold.part_main + (size_t)w * a.fold.nbins;
+                float *gp = a.fold.part_pend + (size_t)w * a.fold.nbins;
+                for (int i = tid; i < a.fold.nbins; i += blockDim.x) {
+                    gm[i] = fw.prof_main[i];
+                    gp[i] = fw.prof_pend[i];
+                }
+            }
+            __syncthreads();
         }
     }
 }
@@ -358,10 +481,10 @@ template <int LOG2N>
 constexpr bool use_pingpong() { return LOG2N <= 12; }
 
 template <int LOG2N>
-size_t dedisp_smem_bytes()
+size_t dedisp_smem_bytes(bool pp)
 {
     using F = FftShape<LOG2N>;
-    return (use_pingpong<LOG2N>() ? 2 : 1) * F::SMEM * sizeof(float2) + (F::N / 2) * sizeof(float);
+    return (pp ? 2 : 1) * F::SMEM * sizeof(float2) + ibuf_floats(F::N / 2) * sizeof(float);
 }
 
 template <int LOG2N>
@@ -397,44 +520,61 @@ static cudaError_t forward_t(InputKind kind, const FwdArgs &a, cudaStream_t st)
     return cudaGetLastError();
 }
 
-template <int LOG2N, bool SERIES, bool FOLD>
-static auto dedisp_fn() { return dedisp_kernel<LOG2N, use_pingpong<LOG2N>(), SERIES, FOLD>; }
+size_t fold_smem_bytes(int nbins, int span_cap, bool smem_prof)
+{
+    return (size_t)span_cap * (2 * sizeof(long long) + 2 * sizeof(int)) +
+           (smem_prof ? 2 * (size_t)nbins * sizeof(float) : 0);
+}
+
+template <int LOG2N, bool PP, bool SERIES, bool FOLD>
+static auto dedisp_fn() { return dedisp_kernel<LOG2N, PP && use_pingpong<LOG2N>(), SERIES, FOLD>; }
+
+// Calls go(kernel) with the instantiation for (pp, series, fold).
+template <int LOG2N, typename G>
+static auto dedisp_select(bool pp, bool series, bool fold, G &&go)
+{
+    if (pp && use_pingpong<LOG2N>()) {
+        if (series && fold)
+            return go(dedisp_fn<LOG2N, true, true, true>());
+        if (fold)
+            return go(dedisp_fn<LOG2N, true, false, true>());
+        return go(dedisp_fn<LOG2N, true, true, false>());
+    }
+    if (series && fold)
+        return go(dedisp_fn<LOG2N, false, true, true>());
+    if (fold)
+        return go(dedisp_fn<LOG2N, false, false, true>());
+    return go(dedisp_fn<LOG2N, false, true, false>());
+}
 
 template <int LOG2N>
-static cudaError_t dedisp_t(bool series, bool fold, const DedispArgs &a, int grid, cudaStream_t st)
+static cudaError_t dedisp_t(bool pp, bool series, bool fold, const DedispArgs &a, int grid, cudaStream_t st)
 {
-    const size_t sm = dedisp_smem_bytes<LOG2N>();
-    auto go = [&](auto k) -> cudaError_t {
+    pp = pp && use_pingpong<LOG2N>();
+    const size_t sm = dedisp_smem_bytes<LOG2N>(pp) +
+                      (fold ? fold_smem_bytes(a.fold.nbins, a.fold.span_cap, a.fold.smem_prof != 0) : 0);
+    return dedisp_select<LOG2N>(pp, series, fold, [&](auto k) -> cudaError_t {
         cudaError_t e = set_smem(k, sm);
         if (e != cudaSuccess)
             return e;
         k<<<grid, FftShape<LOG2N>::T, sm, st>>>(a);
         return cudaGetLastError();
-    };
-    if (series && fold)
-        return go(dedisp_fn<LOG2N, true, true>());
-    if (fold)
-        return go(dedisp_fn<LOG2N, false, true>());
-    return go(dedisp_fn<LOG2N, true, false>());
+    });
 }
 
 template <int LOG2N>
-static int dedisp_occ_t(bool series, bool fold)
+static int dedisp_occ_t(bool pp, bool series, bool fold, size_t extra)
 {
-    const size_t sm = dedisp_smem_bytes<LOG2N>();
-    int n = 0;
-    auto occ = [&](auto k) {
+    pp = pp && use_pingpong<LOG2N>();
+    const size_t sm = dedisp_smem_bytes<LOG2N>(pp) + extra;
+    return dedisp_select<LOG2N>(pp, series, fold, [&](auto k) -> int {
+        int n = 0;
         if (set_smem(k, sm) != cudaSuccess)
-            return;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, FftShape<LOG2N>::T, sm);
-    };
-    if (series && fold)
-        occ(dedisp_fn<LOG2N, true, true>());
-    else if (fold)
-        occ(dedisp_fn<LOG2N, false, true>());
-    else
-        occ(dedisp_fn<LOG2N, true, false>());
-    return n;
+            return 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k, FftShape<LOG2N>::T, sm) != cudaSuccess)
+            return 0;
+        return n;
+    });
 }
 
 template <int LOG2N>
@@ -472,17 +612,18 @@ cudaError_t launch_forward(int log2n, InputKind kind, const FwdArgs &a, cudaStre
     return cudaErrorInvalidValue;
 }
 
-cudaError_t launch_dedisp(int log2n, bool series, bool fold, const DedispArgs &a, int grid, cudaStream_t st)
+cudaError_t launch_dedisp(int log2n, bool pp, bool series, bool fold, const DedispArgs &a, int grid,
+                          cudaStream_t st)
 {
-#define CALL(L) dedisp_t<L>(series, fold, a, grid, st)
+#define CALL(L) dedisp_t<L>(pp, series, fold, a, grid, st)
     MSOSM_DISPATCH(log2n, CALL)
 #undef CALL
     return cudaErrorInvalidValue;
 }
 
-int dedisp_blocks_per_sm(int log2n, bool series, bool fold)
+int dedisp_blocks_per_sm(int log2n, bool pp, bool series, bool fold, size_t extra_smem)
 {
-#define CALL(L) dedisp_occ_t<L>(series, fold)
+#define CALL(L) dedisp_occ_t<L>(pp, series, fold, extra_smem)
     MSOSM_DISPATCH(log2n, CALL)
 #undef CALL
     return 0;

@@ -18,7 +18,7 @@ struct FwdArgs {
     const float2 *hist_in;  // previous call's last M samples
     float2 *hist_out;       // this call's last M samples (for the next call)
     float2 *ring;           // [S][N] spectra
-    int S;
+    int S;                  // ring depth, a power of two
     long long k0;           // global index of this call's first block
     int count;
     const float2 *tw;       // exp(-2 pi i e/N)
@@ -32,11 +32,21 @@ struct FoldArgs {
     int nbins;    // output bins
     int detect;   // 0 |y|^2, 1 |y|
     float *part_main, *part_pend;  // [items][nbins]
+    int smem_prof;  // 1: the work item's profile rows live in shared memory
+    int span_cap;   // spans held in the shared-memory window (>= spans one block can touch)
 };
+
+// intensity staging of one block: M samples, one pad slot per 32
+__host__ __device__ constexpr int ibuf_floats(int m) { return (m + (m >> 5) + 1) & ~1; }
+
+// Extra dynamic shared memory of the folding dedispersion kernel.
+size_t fold_smem_bytes(int nbins, int span_cap, bool smem_prof);
+constexpr int kMaxSmemBins = 4096;
 
 struct DedispArgs {
     const float2 *ring;
-    int S;
+    int S;                    // ring depth, a power of two
+    int max_delay;            // largest block delay of any trial
     long long k0;
     int count;
     int D;
@@ -61,10 +71,12 @@ struct DesignArgs {
 bool log2n_supported(int log2n);
 
 cudaError_t launch_forward(int log2n, InputKind kind, const FwdArgs &a, cudaStream_t st);
-cudaError_t launch_dedisp(int log2n, bool series, bool fold, const DedispArgs &a, int grid,
+// pp: ping-pong shared-memory buffers (one barrier per FFT stage instead of
+// two; twice the buffer space); honoured for FFT sizes up to 4096
+cudaError_t launch_dedisp(int log2n, bool pp, bool series, bool fold, const DedispArgs &a, int grid,
                           cudaStream_t st);
 // CTAs of the dedispersion kernel that fit on one SM (for the persistent grid)
-int dedisp_blocks_per_sm(int log2n, bool series, bool fold);
+int dedisp_blocks_per_sm(int log2n, bool pp, bool series, bool fold, size_t extra_smem);
 cudaError_t launch_design(int log2n, const DesignArgs &a, cudaStream_t st);
 
 cudaError_t launch_fold_reduce(const float *part_main, const float *part_pend, int D, int R, int nbins,
