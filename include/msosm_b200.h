@@ -91,6 +91,29 @@ MSOSM_API msosm_status msosm_prepare_segmentation(float bw, float dm, float f0, 
 MSOSM_API msosm_status msosm_prepare_dedisp_params(float bw, float dm, float f0, unsigned long M,
                                          msosm_complex *H);
 
+/* Allocation-free variant of msosm_prepare_dedisp_params.  No counterpart in
+ * the reference.  For callers that cannot call cudaMalloc: a pipeline that
+ * reserves all of its device memory before an observation and may not
+ * allocate while samples stream in, a host framework whose allocator owns the
+ * device, code that redesigns one trial's filter in the middle of a pass
+ * without the device-wide synchronisation cudaMalloc/cudaFree bring.
+ * The caller passes H_device, a DEVICE buffer of 2M complex values; the
+ * design runs asynchronously on `stream` (a cudaStream_t; NULL = the legacy
+ * default stream) and writes H there, in the reference's scaling.
+ * M: a power of two, 32 <= M <= 8192 (FFT 64..16384 points); anything else
+ * returns MSOSM_ERR_BAD_ARG.  Calls no cudaMalloc, cudaFree or allocating
+ * library routine.  Scratch (twiddle tables, chirp parameters) lives in one
+ * fixed 196,864-byte device array inside the library, which every GPU that
+ * loads the library holds until the process exits.  All calls on a device
+ * share it: calls whose work overlaps on the GPU (two streams, two host
+ * threads) race on it and must be serialised by the caller.  Each call
+ * rewrites every scratch byte it reads, so nothing carries over between
+ * calls.  The first call on a device looks up the array's device address
+ * (cudaGetSymbolAddress, with that device current); make that first call
+ * before any stream capture. */
+MSOSM_API msosm_status msosm_prepare_dedisp_params_noalloc(float bw, float dm, float f0, unsigned long M,
+                                                           msosm_complex *H_device, void *stream);
+
 /* ======================================================================
  * Dedisperser: N DM trials over one input stream
  * ====================================================================== */

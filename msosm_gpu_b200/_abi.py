@@ -76,6 +76,7 @@ def _declare(L: ctypes.CDLL) -> None:
         "msosm_prepare_min_order_osm": (i32, [ul, pul]),
         "msosm_prepare_segmentation": (i32, [f32, f32, f32, ul, pi, vp]),
         "msosm_prepare_dedisp_params": (i32, [f32, f32, f32, ul, vp]),
+        "msosm_prepare_dedisp_params_noalloc": (i32, [f32, f32, f32, ul, vp, vp]),
         "msosm_dedisp_create": (i32, [vp, vp, vp, i32, ul, i32, ul, u32, pvp]),
         "msosm_dedisp_destroy": (i32, [vp]),
         "msosm_dedisp_get_info": (i32, [vp, ctypes.POINTER(DedispInfo)]),

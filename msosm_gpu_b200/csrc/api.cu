@@ -89,6 +89,10 @@ cudaError_t dalloc(T **p, size_t count, size_t &total)
 
 }  // namespace
 
+namespace msosm {
+void set_error_message(const char *msg) { g_err = msg; }
+}  // namespace msosm
+
 struct msosm_dedisp {
     // configuration
     int D = 0, count = 0, log2n = 0, S = 0, R = 1, grid = 1, max_dc = 0, max_delay = 0;

@@ -70,6 +70,9 @@ struct DesignArgs {
 
 bool log2n_supported(int log2n);
 
+// Sets the message msosm_last_error() returns on this thread.
+void set_error_message(const char *msg);
+
 cudaError_t launch_forward(int log2n, InputKind kind, const FwdArgs &a, cudaStream_t st);
 // pp: ping-pong shared-memory buffers (one barrier per FFT stage instead of
 // two; twice the buffer space); honoured for FFT sizes up to 4096
