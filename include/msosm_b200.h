@@ -205,6 +205,45 @@ MSOSM_API msosm_status msosm_dedisp_folded_periods(const msosm_dedisp *d, unsign
 /* Wait for all work of the handle (MSOSM_GPU_DM_concurrent::synchronize). */
 MSOSM_API msosm_status msosm_dedisp_synchronize(msosm_dedisp *d);
 
+/* ======================================================================
+ * Fold_GPU: detection and folding of materialised series
+ * ====================================================================== */
+
+/* Folds a stream of intensities chunk by chunk with the Fold_GPU state
+ * machine (folding/fold_gpu.cpp:48-173) on the device.  size: samples per
+ * chunk; time_bin 0 or (unsigned long)-1 keeps period_samples bins.
+ * Replaces Fold_GPU::Fold_GPU (fold_gpu.cpp:3-27).  Without a discard (or
+ * with Nd = 0) every period is folded; the reference folds nothing then. */
+typedef struct msosm_fold msosm_fold;
+MSOSM_API msosm_status msosm_fold_create(float period, float fs, unsigned long size, unsigned long time_bin,
+                                         msosm_fold **out);
+MSOSM_API msosm_status msosm_fold_destroy(msosm_fold *f);
+/* Fold_GPU::discard_samples (fold_gpu.cpp:29-33): skip ceil(Nd/(period*fs))
+ * periods.  Call before the first msosm_fold_data. */
+MSOSM_API msosm_status msosm_fold_discard_samples(msosm_fold *f, unsigned long Nd);
+/* Intensity sqrt(|a|^2 + |b|^2) of two DEVICE series of size samples (b may
+ * be NULL for one polarisation) into the fold's buffer.  Replaces
+ * Fold_GPU::calculate_intensity (fold_gpu.cpp:35-43) and calculateIntensity
+ * (gpu/gpu_kernel.cu:347-353); the result stays on the device.  The raw
+ * pointers carry no ordering, so this waits for the whole device first; with
+ * dedisperser handles use msosm_fold_calculate_intensity_dedisp. */
+MSOSM_API msosm_status msosm_fold_calculate_intensity(msosm_fold *f, const msosm_complex *a, const msosm_complex *b);
+/* Same from the last series of one or two dedisperser handles (each
+ * count*M == size samples, one trial; b may be NULL), ordered after their
+ * filter calls by events; their next filter call waits for this read. */
+MSOSM_API msosm_status msosm_fold_calculate_intensity_dedisp(msosm_fold *f, msosm_dedisp *a, msosm_dedisp *b);
+/* Load size intensities from a host or device float array instead. */
+MSOSM_API msosm_status msosm_fold_set_intensity(msosm_fold *f, const float *intensity);
+/* Copy the current intensities to host memory (Fold_GPU::total_intensity). */
+MSOSM_API msosm_status msosm_fold_get_intensity(msosm_fold *f, float *out);
+/* Fold the current chunk (Fold_GPU::fold_data, fold_gpu.cpp:48-173). */
+MSOSM_API msosm_status msosm_fold_data(msosm_fold *f);
+/* Folded profile, time_bin floats (Fold_GPU::fold_data_bins, fold_gpu.cpp:175-194). */
+MSOSM_API msosm_status msosm_fold_data_bins(msosm_fold *f, float *out);
+/* period_samples and time_bin as Fold_GPU computes them. */
+MSOSM_API msosm_status msosm_fold_get_shape(const msosm_fold *f, unsigned long *period_samples,
+                                            unsigned long *time_bin);
+
 /* ---- per-stage device timing -------------------------------------------
  * CUDA events recorded on the handle's stream around each stage of every
  * filter call (no effect on results).  Enabling resets the counters;

@@ -176,6 +176,7 @@ public:
 
     int count = 0;
     Complex *output_buffer_d = nullptr;
+    msosm_dedisp *handle() const { return h_.h; }
 
 protected:
     detail::Handle h_;
@@ -418,6 +419,70 @@ private:
     std::vector<float> bw_, dm_, f0_;
     std::vector<detail::Handle> h_;
     std::vector<Complex> out_;
+};
+
+// ---------------------------------------------------------------------------
+// detection + folding (folding/include/fold_gpu.h:10-42)
+// ---------------------------------------------------------------------------
+
+class Fold_GPU {
+public:
+    Fold_GPU(float period, float fs, unsigned long size, std::string outfileName = "fold.txt",
+             unsigned long time_bin = (unsigned long)-1)
+        : size_(size), outfile_(std::move(outfileName))
+    {
+        check(msosm_fold_create(period, fs, size, time_bin, &h_), "msosm_fold_create");
+        check(msosm_fold_get_shape(h_, &period_samples, &this->time_bin), "msosm_fold_get_shape");
+        folded_.assign(this->time_bin, 0.f);
+        folded_data = folded_.data();
+        intensity_.assign(size, 0.f);
+        total_intensity = intensity_.data();
+    }
+    Fold_GPU(const Fold_GPU &) = delete;
+    Fold_GPU &operator=(const Fold_GPU &) = delete;
+    ~Fold_GPU()
+    {
+        if (h_)
+            msosm_fold_destroy(h_);
+    }
+    void discard_samples(unsigned long Nd) { check(msosm_fold_discard_samples(h_, Nd), "discard_samples"); }
+    // MSOSM_GPU_BATCH / OSM_GPU_BATCH: ordered after their last filter call
+    void calculate_intensity(MSOSM_GPU_BATCH *pol1, MSOSM_GPU_BATCH *pol2)
+    {
+        check(msosm_fold_calculate_intensity_dedisp(h_, pol1->handle(), pol2 ? pol2->handle() : nullptr),
+              "calculate_intensity");
+    }
+    // any other class with a device output_buffer_d (waits for the device)
+    template <typename T>
+    void calculate_intensity(T *pol1, T *pol2)
+    {
+        check(msosm_fold_calculate_intensity(h_, pol1->output_buffer_d, pol2 ? pol2->output_buffer_d : nullptr),
+              "calculate_intensity");
+    }
+    // the host total_intensity buffer, after the caller filled it
+    void load_total_intensity() { check(msosm_fold_set_intensity(h_, total_intensity), "set_intensity"); }
+    void fold_data() { check(msosm_fold_data(h_), "fold_data"); }
+    void fold_data_bins() { check(msosm_fold_data_bins(h_, folded_data), "fold_data_bins"); }
+    void write_to_file()
+    {
+        FILE *f = std::fopen(outfile_.c_str(), "w");
+        if (!f)
+            return;
+        for (unsigned long i = 0; i < time_bin; ++i)
+            std::fprintf(f, "%g\n", folded_data[i]);
+        std::fclose(f);
+    }
+
+    float *folded_data = nullptr;
+    unsigned long time_bin = 0;
+    float *total_intensity = nullptr;
+    unsigned long period_samples = 0;
+
+private:
+    msosm_fold *h_ = nullptr;
+    unsigned long size_;
+    std::string outfile_;
+    std::vector<float> folded_, intensity_;
 };
 
 }  // namespace msosm_b200

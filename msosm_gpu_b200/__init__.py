@@ -6,6 +6,7 @@ implemented by the in-tree libmsosm_b200.so.  This package is the Python
 face of that ABI; it has no compute path of its own.
 """
 from ._abi import MsosmError, lib  # noqa: F401
+from .fold import Fold_GPU  # noqa: F401
 from .dedisp import (  # noqa: F401
     Dedisperser,
     MSOSM_GPU_BATCH,
@@ -20,6 +21,7 @@ __all__ = [
     "MSOSM_GPU_DM_concurrent",
     "OSM_GPU_BATCH",
     "OSM_GPU_DM_concurrent",
+    "Fold_GPU",
     "MsosmError",
     "lib",
 ]

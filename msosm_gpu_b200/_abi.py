@@ -96,6 +96,16 @@ def _declare(L: ctypes.CDLL) -> None:
         "msosm_dedisp_synchronize": (i32, [vp]),
         "msosm_dedisp_enable_timing": (i32, [vp, i32]),
         "msosm_dedisp_get_timing": (i32, [vp, ctypes.POINTER(Timing)]),
+        "msosm_fold_create": (i32, [f32, f32, ul, ul, pvp]),
+        "msosm_fold_destroy": (i32, [vp]),
+        "msosm_fold_discard_samples": (i32, [vp, ul]),
+        "msosm_fold_calculate_intensity": (i32, [vp, vp, vp]),
+        "msosm_fold_calculate_intensity_dedisp": (i32, [vp, vp, vp]),
+        "msosm_fold_set_intensity": (i32, [vp, vp]),
+        "msosm_fold_get_intensity": (i32, [vp, vp]),
+        "msosm_fold_data": (i32, [vp]),
+        "msosm_fold_data_bins": (i32, [vp, vp]),
+        "msosm_fold_get_shape": (i32, [vp, pul, pul]),
         "msosm_fold_planner_create": (i32, [f32, f32, ul, pvp]),
         "msosm_fold_planner_destroy": (i32, [vp]),
         "msosm_fold_planner_chunk": (i32, [vp, ul, vp, pull]),

@@ -128,6 +128,12 @@ struct msosm_dedisp {
     int *span_p_d = nullptr, *span_dest_d = nullptr;
     // pinned span staging: [2][cap] of a, b, phase0, dest
     long long *span_host = nullptr;
+    // FFT above one thread block: four-step N = N1*N2, spectra in [k1][k2] order
+    bool large = false;
+    int log2n1 = 0, log2n2 = 0;
+    float2 *lA = nullptr, *lB = nullptr;         // column-pass and row-pass scratch
+    float *lI = nullptr;                         // intensities for folding
+    float2 *tw1f = nullptr, *tw1i = nullptr, *tw2f = nullptr, *tw2i = nullptr;
     // timing: events per timed call: e0 [forward] e1 [fold prep] e2 [dedisp] e3
     // [fold reduce] e6; e4 [h2d] e5 on the copy stream
     bool timing = false;
@@ -151,7 +157,8 @@ void release(msosm_dedisp *d)
         cudaStreamSynchronize(d->copy_stream);
     void *bufs[] = {d->ring, d->H, d->hist, d->series_buf, d->delays_d, d->tw_fwd, d->tw_inv, d->tw_inv_m,
                     d->staging[0], d->staging[1], d->u16_out, d->part_main, d->part_pend, d->prof_out,
-                    d->acc_main, d->acc_pend, d->span_a_d, d->span_b_d, d->span_p_d, d->span_dest_d};
+                    d->acc_main, d->acc_pend, d->span_a_d, d->span_b_d, d->span_p_d, d->span_dest_d,
+                    d->lA, d->lB, d->lI, d->tw1f, d->tw1i, d->tw2f, d->tw2i};
     for (void *p : bufs)
         if (p)
             cudaFree(p);
@@ -236,6 +243,117 @@ cudaError_t plan_grid(msosm_dedisp *d)
     const long long waves = (items + resident - 1) / resident;
     d->grid = (int)((items + waves - 1) / waves);
     return cudaSuccess;
+}
+
+// H of every trial for N above one thread block, in the permuted [k1][k2]
+// order of the four-step spectra, scaled by `scale`:
+//   conj(h) -> FFT_M -> un-permute + conj (= the unnormalised inverse M-point
+//   DFT of h, the reference's h) -> zero pad to N -> FFT_N (permuted).
+msosm_status design_filters_large(int log2n, const std::vector<ChirpParams> &cp, float scale, float2 *Hp,
+                                  cudaStream_t st)
+{
+    const long long N = 1ll << log2n, M = N / 2;
+    const int log2m = log2n - 1;
+    int n1l, n2l, m1l = 0, m2l = 0;
+    large_split(log2n, n1l, n2l);
+    const bool m_large = log2m > kMaxLog2N;
+    if (m_large)
+        large_split(log2m, m1l, m2l);
+    size_t tot = 0;
+    ChirpParams *cp_d = nullptr;
+    float2 *V = nullptr, *W = nullptr, *P = nullptr, *A = nullptr;
+    float2 *twm1 = nullptr, *twm2 = nullptr, *twn1 = nullptr, *twn2 = nullptr;
+    msosm_status s = MSOSM_OK;
+    cudaError_t e = cudaMalloc((void **)&cp_d, sizeof(ChirpParams) * cp.size());
+    if (e == cudaSuccess)
+        e = dalloc(&V, (size_t)M, tot);
+    if (e == cudaSuccess)
+        e = dalloc(&W, (size_t)M, tot);
+    if (e == cudaSuccess)
+        e = dalloc(&P, (size_t)N, tot);
+    if (e == cudaSuccess)
+        e = dalloc(&A, (size_t)N, tot);
+    if (e != cudaSuccess)
+        s = cuda_fail(e, "design scratch");
+    if (s == MSOSM_OK && m_large)
+        s = upload_table(&twm1, 1 << m1l, -1, tot, st);
+    if (s == MSOSM_OK && m_large)
+        s = upload_table(&twm2, 1 << m2l, -1, tot, st);
+    if (s == MSOSM_OK && !m_large)
+        s = upload_table(&twm1, 1 << log2m, -1, tot, st);
+    if (s == MSOSM_OK)
+        s = upload_table(&twn1, 1 << n1l, -1, tot, st);
+    if (s == MSOSM_OK)
+        s = upload_table(&twn2, 1 << n2l, -1, tot, st);
+    if (s == MSOSM_OK) {
+        e = cudaMemcpyAsync(cp_d, cp.data(), sizeof(ChirpParams) * cp.size(), cudaMemcpyHostToDevice, st);
+        for (size_t i = 0; i < cp.size() && e == cudaSuccess; ++i) {
+            e = launch_chirp_conj(cp_d + i, V, M, -1, st);
+            if (e != cudaSuccess)
+                break;
+            if (m_large) {
+                LargeColArgs ca{};
+                ca.input = V;
+                ca.out = A;
+                ca.N = M;
+                ca.N2 = 1ll << m2l;
+                ca.len = M;
+                ca.log2n = log2m;
+                ca.count = 1;
+                ca.tw1 = twm1;
+                e = launch_large_col_fwd(m1l, 2, ca, 1, st);
+                if (e == cudaSuccess) {
+                    LargeRowArgs ra{};
+                    ra.in = A;
+                    ra.out = W;
+                    ra.N = M;
+                    ra.log2n = log2m;
+                    ra.tw2 = twm2;
+                    ra.count = 1;
+                    e = launch_large_row(m2l, 2, ra, 1 << m1l, 1, 1, st);
+                }
+                if (e == cudaSuccess)
+                    e = launch_unpermute_conj(W, P, M, 1ll << m1l, 1ll << m2l, N, st);
+            } else {
+                e = launch_vec_fft(log2m, -1, V, W, twm1, 1, st);
+                if (e == cudaSuccess)
+                    e = launch_unpermute_conj(W, P, M, 1, M, N, st);
+            }
+            if (e == cudaSuccess) {
+                LargeColArgs ca{};
+                ca.input = P;
+                ca.out = A;
+                ca.N = N;
+                ca.N2 = 1ll << n2l;
+                ca.len = N;
+                ca.log2n = log2n;
+                ca.count = 1;
+                ca.tw1 = twn1;
+                e = launch_large_col_fwd(n1l, 2, ca, 1, st);
+            }
+            if (e == cudaSuccess) {
+                LargeRowArgs ra{};
+                ra.in = A;
+                ra.out = Hp + i * (size_t)N;
+                ra.N = N;
+                ra.log2n = log2n;
+                ra.tw2 = twn2;
+                ra.count = 1;
+                e = launch_large_row(n2l, 2, ra, 1 << n1l, 1, 1, st);
+            }
+            if (e == cudaSuccess)
+                e = launch_conj_scale(Hp + i * (size_t)N, N, scale, 0, st);
+        }
+        if (e == cudaSuccess)
+            e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess)
+            s = cuda_fail(e, "large filter design");
+    }
+    void *bufs[] = {cp_d, V, W, P, A, twm1, twm2, twn1, twn2};
+    for (void *b : bufs)
+        if (b)
+            cudaFree(b);
+    return s;
 }
 
 msosm_status check_handle(const msosm_dedisp *d)
@@ -378,10 +496,11 @@ msosm_status msosm_dedisp_create(const float *bw, const float *dm, const float *
         release(d);
         return fail(MSOSM_ERR_BAD_ARG, "FFT size %lu is not a power of two", 2 * M);
     }
-    if (!log2n_supported(log2n)) {
+    if (!log2n_supported(log2n) && !large_supported(log2n)) {
         release(d);
-        return fail(MSOSM_ERR_UNSUPPORTED, "FFT size %lu outside the supported 64..16384", 2 * M);
+        return fail(MSOSM_ERR_UNSUPPORTED, "FFT size %lu outside the supported 64..2^24", 2 * M);
     }
+    d->large = !log2n_supported(log2n);
     if (input_size != 0)
         count = (int)(input_size / M);
     if (count < 1) {
@@ -454,29 +573,53 @@ msosm_status msosm_dedisp_create(const float *bw, const float *dm, const float *
         CKD(dalloc((float2 **)&d->staging[i], (size_t)count * M, tot));
     if (d->series)
         CKD(dalloc(&d->series_buf, (size_t)numDMs * count * M + 1, tot));
+    if (d->large)
+        large_split(log2n, d->log2n1, d->log2n2);
     {
+        // per-bin delays on the device; for the four-step layout permuted to
+        // position k1*N2 + k2 of bin k1 + N1*k2
         std::vector<uint16_t> dl(d->delays.size());
-        for (size_t i = 0; i < dl.size(); ++i)
-            dl[i] = (uint16_t)d->delays[i];
+        const unsigned long N1 = 1ul << d->log2n1, N2 = 1ul << d->log2n2;
+        for (int t = 0; t < numDMs; ++t)
+            for (unsigned long p = 0; p < N; ++p) {
+                const unsigned long b = d->large ? (p / N2) + N1 * (p % N2) : p;
+                dl[(size_t)t * N + p] = (uint16_t)d->delays[(size_t)t * N + b];
+            }
         CKD(cudaMemcpy(d->delays_d, dl.data(), sizeof(uint16_t) * dl.size(), cudaMemcpyHostToDevice));
     }
     msosm_status s;
-    if ((s = upload_table(&d->tw_fwd, (int)N, -1, tot, d->stream)) != MSOSM_OK ||
-        (s = upload_table(&d->tw_inv, (int)N, +1, tot, d->stream)) != MSOSM_OK ||
-        (s = upload_table(&d->tw_inv_m, (int)M, +1, tot, d->stream)) != MSOSM_OK) {
-        release(d);
-        return s;
-    }
     std::vector<ChirpParams> cp(numDMs);
     for (int i = 0; i < numDMs; ++i)
         cp[i] = chirp_params(bw[i], dm[i], f0[i], M);
     // 1/N^2: the reference's /N before and /(2M) after the inverse FFT
     const float scale = 1.0f / ((float)N * (float)N);
-    if ((s = design_filters(log2n, cp, scale, -1, d->tw_inv_m, d->tw_fwd, d->H, d->stream)) != MSOSM_OK) {
-        release(d);
-        return s;
+    if (!d->large) {
+        if ((s = upload_table(&d->tw_fwd, (int)N, -1, tot, d->stream)) != MSOSM_OK ||
+            (s = upload_table(&d->tw_inv, (int)N, +1, tot, d->stream)) != MSOSM_OK ||
+            (s = upload_table(&d->tw_inv_m, (int)M, +1, tot, d->stream)) != MSOSM_OK) {
+            release(d);
+            return s;
+        }
+        if ((s = design_filters(log2n, cp, scale, -1, d->tw_inv_m, d->tw_fwd, d->H, d->stream)) != MSOSM_OK) {
+            release(d);
+            return s;
+        }
+        CKD(plan_grid(d));
+    } else {
+        if ((s = upload_table(&d->tw1f, 1 << d->log2n1, -1, tot, d->stream)) != MSOSM_OK ||
+            (s = upload_table(&d->tw1i, 1 << d->log2n1, +1, tot, d->stream)) != MSOSM_OK ||
+            (s = upload_table(&d->tw2f, 1 << d->log2n2, -1, tot, d->stream)) != MSOSM_OK ||
+            (s = upload_table(&d->tw2i, 1 << d->log2n2, +1, tot, d->stream)) != MSOSM_OK) {
+            release(d);
+            return s;
+        }
+        CKD(dalloc(&d->lA, (size_t)count * N, tot));
+        CKD(dalloc(&d->lB, (size_t)numDMs * count * N, tot));
+        if ((s = design_filters_large(log2n, cp, scale, d->H, d->stream)) != MSOSM_OK) {
+            release(d);
+            return s;
+        }
     }
-    CKD(plan_grid(d));
 #undef CKD
     *out = d;
     return MSOSM_OK;
@@ -536,11 +679,15 @@ msosm_status msosm_dedisp_get_dedisp_params(const msosm_dedisp *d, int i, msosm_
     if (check_handle(d) || !H || i < 0 || i >= d->D)
         return fail(MSOSM_ERR_BAD_ARG, "bad trial index or null output");
     CK(cudaStreamSynchronize(d->stream));
-    CK(cudaMemcpy(H, d->H + (size_t)i * d->N, sizeof(float2) * d->N, cudaMemcpyDeviceToHost));
+    std::vector<msosm_complex> tmp(d->N);
+    CK(cudaMemcpy(tmp.data(), d->H + (size_t)i * d->N, sizeof(float2) * d->N, cudaMemcpyDeviceToHost));
     const float up = (float)d->N * (float)d->N;  // undo the 1/N^2 (a power of two: exact)
+    const unsigned long N1 = 1ul << d->log2n1, N2 = 1ul << d->log2n2;
     for (unsigned long b = 0; b < d->N; ++b) {
-        H[b].x *= up;
-        H[b].y *= up;
+        // four-step layout: bin b = k1 + N1*k2 sits at k1*N2 + k2
+        const unsigned long p = d->large ? (b % N1) * N2 + b / N1 : b;
+        H[b].x = tmp[p].x * up;
+        H[b].y = tmp[p].y * up;
     }
     return MSOSM_OK;
 }
@@ -551,6 +698,130 @@ msosm_status msosm_dedisp_set_stream(msosm_dedisp *d, void *stream)
         return MSOSM_ERR_BAD_ARG;
     CK(cudaStreamSynchronize(d->stream));
     d->stream = stream ? (cudaStream_t)stream : d->own_stream;
+    return MSOSM_OK;
+}
+
+// fold bookkeeping shared by both layouts: plan this call's spans, upload
+// them, flush a pending period that completes now, clear the partial rows
+static msosm_status fold_prepare(msosm_dedisp *d, int sb, FoldArgs &fa)
+{
+    bool flush = false;
+    d->planner->chunk((unsigned long)d->count * d->M, d->spans, flush);
+    const int n = (int)d->spans.size();
+    if (n > d->span_cap)
+        return fail(MSOSM_ERR_STATE, "fold planner produced %d spans (capacity %d)", n, d->span_cap);
+    // reuse of the pinned span staging: wait for its copy two calls ago
+    CK(cudaEventSynchronize(d->ev_spans[sb]));
+    long long *h = d->span_host + (size_t)sb * 4 * d->span_cap;
+    int *hp = reinterpret_cast<int *>(h + 2 * d->span_cap);
+    for (int i = 0; i < n; ++i) {
+        h[i] = d->spans[i].a;
+        h[d->span_cap + i] = d->spans[i].b;
+        hp[i] = d->spans[i].phase0;
+        hp[d->span_cap + i] = d->spans[i].dest;
+    }
+    CK(cudaMemcpyAsync(d->span_a_d, h, sizeof(long long) * n, cudaMemcpyHostToDevice, d->stream));
+    CK(cudaMemcpyAsync(d->span_b_d, h + d->span_cap, sizeof(long long) * n, cudaMemcpyHostToDevice, d->stream));
+    CK(cudaMemcpyAsync(d->span_p_d, hp, sizeof(int) * n, cudaMemcpyHostToDevice, d->stream));
+    CK(cudaMemcpyAsync(d->span_dest_d, hp + d->span_cap, sizeof(int) * n, cudaMemcpyHostToDevice, d->stream));
+    CK(cudaEventRecord(d->ev_spans[sb], d->stream));
+    if (flush) {
+        CK(launch_fold_flush(d->acc_main, d->acc_pend, (size_t)d->D * d->nbins, d->stream));
+        d->launches += 1;
+    }
+    const size_t prow = (size_t)d->D * d->R * d->nbins;
+    CK(cudaMemsetAsync(d->part_main, 0, sizeof(float) * prow, d->stream));
+    CK(cudaMemsetAsync(d->part_pend, 0, sizeof(float) * prow, d->stream));
+    fa.span_a = d->span_a_d;
+    fa.span_b = d->span_b_d;
+    fa.span_phase0 = d->span_p_d;
+    fa.span_dest = d->span_dest_d;
+    fa.nspans = n;
+    fa.bpt = d->bpt;
+    fa.nbins = d->nbins;
+    fa.detect = d->detect;
+    fa.part_main = d->part_main;
+    fa.part_pend = d->part_pend;
+    fa.smem_prof = d->nbins <= kMaxSmemBins ? 1 : 0;
+    fa.span_cap = d->win_cap;
+    return MSOSM_OK;
+}
+
+// One call with the four-step layout: column + row forward passes into the
+// ring, then per trial the gathering inverse row pass and the pruned inverse
+// column pass; folding runs over the materialised intensities.
+static msosm_status filter_block_large(msosm_dedisp *d, const void *src, InputKind kind,
+                                       msosm_dedisp::CallEvents *ev, unsigned long long launches0)
+{
+    const int sb = (int)(d->calls & 1);
+    const long long N = (long long)d->N;
+    LargeColArgs ca{};
+    ca.input = src;
+    ca.hist_in = d->hist + (size_t)(d->calls & 1) * d->M;
+    ca.hist_out = d->hist + (size_t)((d->calls + 1) & 1) * d->M;
+    ca.out = d->lA;
+    ca.N = N;
+    ca.N2 = 1ll << d->log2n2;
+    ca.log2n = d->log2n;
+    ca.count = d->count;
+    ca.tw1 = d->tw1f;
+    if (ev)
+        CK(cudaEventRecord(ev->e[0], d->stream));
+    CK(launch_large_col_fwd(d->log2n1, kind, ca, d->count, d->stream));
+    LargeRowArgs ra{};
+    ra.in = d->lA;
+    ra.ring = d->ring;
+    ra.S = d->S;
+    ra.k0 = (long long)d->calls * d->count;
+    ra.count = d->count;
+    ra.N = N;
+    ra.log2n = d->log2n;
+    ra.tw2 = d->tw2f;
+    CK(launch_large_row(d->log2n2, 0, ra, 1 << d->log2n1, d->count, 1, d->stream));
+    d->launches += 2;
+    CK(cudaEventRecord(d->ev_consumed[sb], d->stream));
+    if (ev)
+        CK(cudaEventRecord(ev->e[1], d->stream));
+    FoldArgs fa{};
+    if (d->fold) {
+        msosm_status s = fold_prepare(d, sb, fa);
+        if (s != MSOSM_OK)
+            return s;
+    }
+    if (ev)
+        CK(cudaEventRecord(ev->e[2], d->stream));
+    ra.out = d->lB;
+    ra.H = d->H;
+    ra.delays = d->delays_d;
+    ra.tw2 = d->tw2i;
+    CK(launch_large_row(d->log2n2, 1, ra, 1 << d->log2n1, d->count, d->D, d->stream));
+    LargeColArgs ia{};
+    ia.in = d->lB;
+    ia.N = N;
+    ia.N2 = 1ll << d->log2n2;
+    ia.log2n = d->log2n;
+    ia.count = d->count;
+    ia.tw1 = d->tw1i;
+    ia.series = d->series_buf;
+    ia.intensity = d->fold ? d->lI : nullptr;
+    ia.detect = d->detect;
+    CK(launch_large_col_inv(d->log2n1, ia, d->count, d->D, d->stream));
+    d->launches += 2;
+    if (ev)
+        CK(cudaEventRecord(ev->e[3], d->stream));
+    if (d->fold) {
+        CK(launch_fold_series(d->lI, (long long)d->count * d->M, d->R, fa, d->grid, d->D, d->stream));
+        CK(launch_fold_reduce(d->part_main, d->part_pend, d->D, d->R, d->nbins, d->acc_main, d->acc_pend,
+                              d->stream));
+        d->launches += 2;
+    }
+    if (d->series)
+        CK(cudaMemsetAsync(d->series_buf + (size_t)d->D * d->count * d->M, 0, sizeof(float2), d->stream));
+    if (ev) {
+        CK(cudaEventRecord(ev->e[6], d->stream));
+        d->timed_launches += d->launches - launches0;
+    }
+    d->calls += 1;
     return MSOSM_OK;
 }
 
@@ -588,6 +859,8 @@ static msosm_status filter_block(msosm_dedisp *d, const void *input, InputKind k
         CK(cudaStreamWaitEvent(d->stream, d->ev_copied[sb], 0));
         src = d->staging[sb];
     }
+    if (d->large)
+        return filter_block_large(d, src, kind, ev, launches0);
     FwdArgs fa;
     fa.input = src;
     fa.hist_in = d->hist + (size_t)(d->calls & 1) * d->M;
@@ -619,46 +892,9 @@ static msosm_status filter_block(msosm_dedisp *d, const void *input, InputKind k
     da.series = d->series_buf;
     da.fold.nspans = -1;
     if (d->fold) {
-        bool flush = false;
-        d->planner->chunk((unsigned long)d->count * d->M, d->spans, flush);
-        const int n = (int)d->spans.size();
-        if (n > d->span_cap)
-            return fail(MSOSM_ERR_STATE, "fold planner produced %d spans (capacity %d)", n, d->span_cap);
-        // reuse of the pinned span staging: wait for its copy two calls ago
-        CK(cudaEventSynchronize(d->ev_spans[sb]));
-        long long *h = d->span_host + (size_t)sb * 4 * d->span_cap;
-        for (int i = 0; i < n; ++i) {
-            h[i] = d->spans[i].a;
-            h[d->span_cap + i] = d->spans[i].b;
-            int *hp = reinterpret_cast<int *>(h + 2 * d->span_cap);
-            hp[i] = d->spans[i].phase0;
-            hp[d->span_cap + i] = d->spans[i].dest;
-        }
-        CK(cudaMemcpyAsync(d->span_a_d, h, sizeof(long long) * n, cudaMemcpyHostToDevice, d->stream));
-        CK(cudaMemcpyAsync(d->span_b_d, h + d->span_cap, sizeof(long long) * n, cudaMemcpyHostToDevice, d->stream));
-        const int *hp = reinterpret_cast<const int *>(h + 2 * d->span_cap);
-        CK(cudaMemcpyAsync(d->span_p_d, hp, sizeof(int) * n, cudaMemcpyHostToDevice, d->stream));
-        CK(cudaMemcpyAsync(d->span_dest_d, hp + d->span_cap, sizeof(int) * n, cudaMemcpyHostToDevice, d->stream));
-        CK(cudaEventRecord(d->ev_spans[sb], d->stream));
-        if (flush) {
-            CK(launch_fold_flush(d->acc_main, d->acc_pend, (size_t)d->D * d->nbins, d->stream));
-            d->launches += 1;
-        }
-        const size_t prow = (size_t)d->D * d->R * d->nbins;
-        CK(cudaMemsetAsync(d->part_main, 0, sizeof(float) * prow, d->stream));
-        CK(cudaMemsetAsync(d->part_pend, 0, sizeof(float) * prow, d->stream));
-        da.fold.span_a = d->span_a_d;
-        da.fold.span_b = d->span_b_d;
-        da.fold.span_phase0 = d->span_p_d;
-        da.fold.span_dest = d->span_dest_d;
-        da.fold.nspans = n;
-        da.fold.bpt = d->bpt;
-        da.fold.nbins = d->nbins;
-        da.fold.detect = d->detect;
-        da.fold.part_main = d->part_main;
-        da.fold.part_pend = d->part_pend;
-        da.fold.smem_prof = d->nbins <= kMaxSmemBins ? 1 : 0;
-        da.fold.span_cap = d->win_cap;
+        msosm_status st = fold_prepare(d, sb, da.fold);
+        if (st != MSOSM_OK)
+            return st;
     }
     // the partial-row clears and the flush above belong to the fold time;
     // the dedispersion kernel is timed alone
@@ -764,15 +1000,28 @@ msosm_status msosm_dedisp_fold_init(msosm_dedisp *d, float period, float fs, uns
     if (d->win_cap < 64)
         d->win_cap = 64;
     d->fold = true;
-    {
+    if (!d->large) {
         cudaError_t e = plan_grid(d);
         if (e != cudaSuccess) {
             d->fold = false;
             return cuda_fail(e, "plan_grid");
         }
+    } else {
+        // the series fold: ranges of 2048-sample blocks per trial, about four
+        // thread blocks per SM over all trials
+        int dev = 0, sms = 0;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const long long nblk = ((long long)d->count * d->M + fold_series_block() - 1) / fold_series_block();
+        long long R = (4ll * (sms > 0 ? sms : 1) + d->D - 1) / d->D;
+        R = R > nblk ? nblk : (R < 1 ? 1 : R);
+        d->R = (int)R;
+        d->grid = (int)R;
     }
     d->fold = false;
     size_t &tot = d->device_bytes;
+    if (d->large)
+        CK(dalloc(&d->lI, (size_t)d->D * d->count * d->M, tot));
     const size_t prow = (size_t)d->D * d->R * d->nbins;
     const size_t nacc = (size_t)d->D * d->nbins;
     CK(dalloc(&d->part_main, prow, tot));
@@ -859,6 +1108,275 @@ msosm_status msosm_dedisp_get_timing(msosm_dedisp *d, msosm_timing *t)
     }
     t->calls = d->timed.size();
     t->kernel_launches = d->timed_launches;
+    return MSOSM_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Fold_GPU
+// ---------------------------------------------------------------------------
+
+struct msosm_fold {
+    unsigned long size = 0, ps = 0;
+    int nbins = 0, bpt = 1, span_cap = 0, win_cap = 64, R = 1, grid = 1;
+    double out_scale = 1.0;
+    float period = 0.f, fs = 0.f;
+    FoldPlanner *planner = nullptr;
+    bool started = false;
+    std::vector<FoldSpan> spans;
+    cudaStream_t stream = nullptr;
+    float *I = nullptr, *part_main = nullptr, *part_pend = nullptr, *prof_out = nullptr;
+    double *acc_main = nullptr, *acc_pend = nullptr;
+    long long *span_a = nullptr, *span_b = nullptr;
+    int *span_p = nullptr, *span_dest = nullptr;
+    long long *span_host = nullptr;
+};
+
+static void fold_release(msosm_fold *f)
+{
+    if (!f)
+        return;
+    if (f->stream)
+        cudaStreamSynchronize(f->stream);
+    void *bufs[] = {f->I, f->part_main, f->part_pend, f->prof_out, f->acc_main, f->acc_pend,
+                    f->span_a, f->span_b, f->span_p, f->span_dest};
+    for (void *p : bufs)
+        if (p)
+            cudaFree(p);
+    if (f->span_host)
+        cudaFreeHost(f->span_host);
+    if (f->stream)
+        cudaStreamDestroy(f->stream);
+    delete f->planner;
+    delete f;
+}
+
+msosm_status msosm_fold_create(float period, float fs, unsigned long size, unsigned long time_bin, msosm_fold **out)
+{
+    if (!out || !(period > 0) || !(fs > 0) || size == 0)
+        return fail(MSOSM_ERR_BAD_ARG, "msosm_fold_create: period, fs and size must be positive");
+    *out = nullptr;
+    if (msosm_device_count() == 0)
+        return fail(MSOSM_ERR_NO_DEVICE, "no CUDA device");
+    msosm_fold *f = new (std::nothrow) msosm_fold;
+    if (!f)
+        return fail(MSOSM_ERR_OOM, "host allocation");
+    f->period = period;
+    f->fs = fs;
+    f->size = size;
+    // period_samples as fold_gpu.cpp:5-7 computes it
+    const float psf = period * fs;
+    f->ps = (unsigned long)psf;
+    if (f->ps == 0 || f->ps > (1ul << 30)) {
+        fold_release(f);
+        return fail(MSOSM_ERR_BAD_ARG, "period*fs gives %lu samples", f->ps);
+    }
+    const unsigned long nb = (time_bin == 0 || time_bin == (unsigned long)-1) ? f->ps : time_bin;
+    if (nb > f->ps) {
+        fold_release(f);
+        return fail(MSOSM_ERR_BAD_ARG, "time_bin %lu exceeds period_samples %lu", time_bin, f->ps);
+    }
+    f->nbins = (int)nb;
+    f->bpt = nb == f->ps ? 1 : (int)(f->ps / nb);
+    f->out_scale = nb == f->ps ? 1.0 : 1.0 / (double)f->bpt;
+    f->span_cap = (int)(size / f->ps) + 8;
+    f->win_cap = (int)((unsigned long)fold_series_block() / f->ps) + 4;
+    if (f->win_cap < 64)
+        f->win_cap = 64;
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const long long blocks = ((long long)size + fold_series_block() - 1) / fold_series_block();
+    long long R = 4ll * (sms > 0 ? sms : 1);
+    if (R > blocks)
+        R = blocks;
+    f->R = (int)(R < 1 ? 1 : R);
+    f->grid = f->R;
+    size_t tot = 0;
+#define CKF(call)                                                                                      \
+    do {                                                                                               \
+        cudaError_t e_ = (call);                                                                       \
+        if (e_ != cudaSuccess) {                                                                       \
+            msosm_status s_ = cuda_fail(e_, #call);                                                    \
+            fold_release(f);                                                                           \
+            return s_;                                                                                 \
+        }                                                                                              \
+    } while (0)
+    CKF(cudaStreamCreateWithFlags(&f->stream, cudaStreamNonBlocking));
+    CKF(dalloc(&f->I, size, tot));
+    CKF(dalloc(&f->part_main, (size_t)f->R * f->nbins, tot));
+    CKF(dalloc(&f->part_pend, (size_t)f->R * f->nbins, tot));
+    CKF(dalloc(&f->acc_main, (size_t)f->nbins, tot));
+    CKF(dalloc(&f->acc_pend, (size_t)f->nbins, tot));
+    CKF(dalloc(&f->prof_out, (size_t)f->nbins, tot));
+    CKF(dalloc(&f->span_a, (size_t)f->span_cap, tot));
+    CKF(dalloc(&f->span_b, (size_t)f->span_cap, tot));
+    CKF(dalloc(&f->span_p, (size_t)f->span_cap, tot));
+    CKF(dalloc(&f->span_dest, (size_t)f->span_cap, tot));
+    CKF(cudaMallocHost((void **)&f->span_host, sizeof(long long) * 4 * f->span_cap));
+    CKF(cudaMemsetAsync(f->acc_main, 0, sizeof(double) * f->nbins, f->stream));
+    CKF(cudaMemsetAsync(f->acc_pend, 0, sizeof(double) * f->nbins, f->stream));
+    CKF(cudaMemsetAsync(f->I, 0, sizeof(float) * size, f->stream));
+    CKF(cudaStreamSynchronize(f->stream));
+#undef CKF
+    f->planner = new (std::nothrow) FoldPlanner(period, fs, 0, true);
+    if (!f->planner) {
+        fold_release(f);
+        return fail(MSOSM_ERR_OOM, "host allocation");
+    }
+    *out = f;
+    return MSOSM_OK;
+}
+
+msosm_status msosm_fold_destroy(msosm_fold *f)
+{
+    fold_release(f);
+    return MSOSM_OK;
+}
+
+msosm_status msosm_fold_discard_samples(msosm_fold *f, unsigned long Nd)
+{
+    if (!f)
+        return fail(MSOSM_ERR_BAD_ARG, "null handle");
+    if (f->started)
+        return fail(MSOSM_ERR_STATE, "discard_samples after the first fold_data");
+    FoldPlanner *p = new (std::nothrow) FoldPlanner(f->period, f->fs, Nd, true);
+    if (!p)
+        return fail(MSOSM_ERR_OOM, "host allocation");
+    delete f->planner;
+    f->planner = p;
+    return MSOSM_OK;
+}
+
+msosm_status msosm_fold_calculate_intensity(msosm_fold *f, const msosm_complex *a, const msosm_complex *b)
+{
+    if (!f || !a)
+        return fail(MSOSM_ERR_BAD_ARG, "null argument");
+    if (!is_device_ptr(a) || (b && !is_device_ptr(b)))
+        return fail(MSOSM_ERR_BAD_ARG, "calculate_intensity takes device series (e.g. output_buffer_d)");
+    // the producer of a and b is unknown: wait for all prior device work
+    CK(cudaDeviceSynchronize());
+    CK(launch_intensity(reinterpret_cast<const float2 *>(a), reinterpret_cast<const float2 *>(b), f->I, f->size,
+                        f->stream));
+    return MSOSM_OK;
+}
+
+msosm_status msosm_fold_calculate_intensity_dedisp(msosm_fold *f, msosm_dedisp *a, msosm_dedisp *b)
+{
+    if (!f || !a)
+        return fail(MSOSM_ERR_BAD_ARG, "null argument");
+    msosm_dedisp *hs[2] = {a, b};
+    for (msosm_dedisp *d : hs) {
+        if (!d)
+            continue;
+        if (!d->series)
+            return fail(MSOSM_ERR_STATE, "handle created with MSOSM_FLAG_NO_SERIES");
+        if ((unsigned long)d->count * d->M != f->size || d->D != 1)
+            return fail(MSOSM_ERR_BAD_ARG, "series of %d trial(s) x %lu samples, fold chunk is %lu samples", d->D,
+                        (unsigned long)d->count * d->M, f->size);
+    }
+    cudaEvent_t ev;
+    CK(cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+    cudaError_t e = cudaSuccess;
+    for (msosm_dedisp *d : hs)
+        if (d && e == cudaSuccess) {
+            e = cudaEventRecord(ev, d->stream);
+            if (e == cudaSuccess)
+                e = cudaStreamWaitEvent(f->stream, ev, 0);
+        }
+    if (e == cudaSuccess)
+        e = launch_intensity(a->series_buf, b ? b->series_buf : nullptr, f->I, f->size, f->stream);
+    // the handles' next calls overwrite their series: order them after this read
+    if (e == cudaSuccess)
+        e = cudaEventRecord(ev, f->stream);
+    for (msosm_dedisp *d : hs)
+        if (d && e == cudaSuccess)
+            e = cudaStreamWaitEvent(d->stream, ev, 0);
+    cudaEventDestroy(ev);
+    if (e != cudaSuccess)
+        return cuda_fail(e, "calculate_intensity");
+    return MSOSM_OK;
+}
+
+msosm_status msosm_fold_set_intensity(msosm_fold *f, const float *intensity)
+{
+    if (!f || !intensity)
+        return fail(MSOSM_ERR_BAD_ARG, "null argument");
+    CK(cudaMemcpyAsync(f->I, intensity, sizeof(float) * f->size, cudaMemcpyDefault, f->stream));
+    CK(cudaStreamSynchronize(f->stream));
+    return MSOSM_OK;
+}
+
+msosm_status msosm_fold_get_intensity(msosm_fold *f, float *out)
+{
+    if (!f || !out)
+        return fail(MSOSM_ERR_BAD_ARG, "null argument");
+    CK(cudaMemcpyAsync(out, f->I, sizeof(float) * f->size, cudaMemcpyDefault, f->stream));
+    CK(cudaStreamSynchronize(f->stream));
+    return MSOSM_OK;
+}
+
+msosm_status msosm_fold_data(msosm_fold *f)
+{
+    if (!f)
+        return fail(MSOSM_ERR_BAD_ARG, "null handle");
+    f->started = true;
+    bool flush = false;
+    f->planner->chunk(f->size, f->spans, flush);
+    const int n = (int)f->spans.size();
+    if (n > f->span_cap)
+        return fail(MSOSM_ERR_STATE, "fold planner produced %d spans (capacity %d)", n, f->span_cap);
+    long long *h = f->span_host;
+    int *hp = reinterpret_cast<int *>(h + 2 * f->span_cap);
+    for (int i = 0; i < n; ++i) {
+        h[i] = f->spans[i].a;
+        h[f->span_cap + i] = f->spans[i].b;
+        hp[i] = f->spans[i].phase0;
+        hp[f->span_cap + i] = f->spans[i].dest;
+    }
+    CK(cudaMemcpyAsync(f->span_a, h, sizeof(long long) * n, cudaMemcpyHostToDevice, f->stream));
+    CK(cudaMemcpyAsync(f->span_b, h + f->span_cap, sizeof(long long) * n, cudaMemcpyHostToDevice, f->stream));
+    CK(cudaMemcpyAsync(f->span_p, hp, sizeof(int) * n, cudaMemcpyHostToDevice, f->stream));
+    CK(cudaMemcpyAsync(f->span_dest, hp + f->span_cap, sizeof(int) * n, cudaMemcpyHostToDevice, f->stream));
+    if (flush)
+        CK(launch_fold_flush(f->acc_main, f->acc_pend, (size_t)f->nbins, f->stream));
+    CK(cudaMemsetAsync(f->part_main, 0, sizeof(float) * f->R * f->nbins, f->stream));
+    CK(cudaMemsetAsync(f->part_pend, 0, sizeof(float) * f->R * f->nbins, f->stream));
+    FoldArgs a;
+    a.span_a = f->span_a;
+    a.span_b = f->span_b;
+    a.span_phase0 = f->span_p;
+    a.span_dest = f->span_dest;
+    a.nspans = n;
+    a.bpt = f->bpt;
+    a.nbins = f->nbins;
+    a.detect = 0;
+    a.part_main = f->part_main;
+    a.part_pend = f->part_pend;
+    a.smem_prof = f->nbins <= kMaxSmemBins ? 1 : 0;
+    a.span_cap = f->win_cap;
+    CK(launch_fold_series(f->I, (long long)f->size, f->R, a, f->grid, 1, f->stream));
+    CK(launch_fold_reduce(f->part_main, f->part_pend, 1, f->R, f->nbins, f->acc_main, f->acc_pend, f->stream));
+    // the pinned span staging is reused by the next call
+    CK(cudaStreamSynchronize(f->stream));
+    return MSOSM_OK;
+}
+
+msosm_status msosm_fold_data_bins(msosm_fold *f, float *out)
+{
+    if (!f || !out)
+        return fail(MSOSM_ERR_BAD_ARG, "null argument");
+    CK(launch_fold_readout(f->acc_main, (size_t)f->nbins, f->out_scale, f->prof_out, f->stream));
+    CK(cudaMemcpyAsync(out, f->prof_out, sizeof(float) * f->nbins, cudaMemcpyDeviceToHost, f->stream));
+    CK(cudaStreamSynchronize(f->stream));
+    return MSOSM_OK;
+}
+
+msosm_status msosm_fold_get_shape(const msosm_fold *f, unsigned long *period_samples, unsigned long *time_bin)
+{
+    if (!f || !period_samples || !time_bin)
+        return fail(MSOSM_ERR_BAD_ARG, "null argument");
+    *period_samples = f->ps;
+    *time_bin = (unsigned long)f->nbins;
     return MSOSM_OK;
 }
 

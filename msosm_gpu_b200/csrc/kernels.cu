@@ -25,6 +25,7 @@
 // for bin b, the product of block k - delay[b] (zero before the stream
 // start).  Here the ring holds the input spectra once for all trials and
 // each trial gathers X[k - delay[b]][b] * H[b] directly.
+#include "chirp.cuh"
 #include "fft_smem.cuh"
 #include "kernels.hpp"
 
@@ -320,48 +321,80 @@ __global__ void __launch_bounds__(FftShape<LOG2N>::T) dedisp_kernel(DedispArgs a
 }
 
 // ---------------------------------------------------------------------------
-// filter design on the device
+// folding of a materialised intensity series (Fold_GPU)
 // ---------------------------------------------------------------------------
 
-// Chirp phase at offset index i with the reference's rounding sequence
-// (msosm_prepare.cpp:50-62): float w, float (w + w0), the rest in double,
-// left to right.  Explicit round-to-nearest intrinsics keep the compiler
-// from contracting any step into an FMA.
-__device__ __forceinline__ double chirp_phase(const ChirpParams &p, unsigned int i)
+// sqrt(|a|^2 + |b|^2) per sample (b may be null): gpu/gpu_kernel.cu:347-353.
+__global__ void intensity_kernel(const float2 *__restrict__ a, const float2 *__restrict__ b, float *__restrict__ out,
+                                 size_t n)
 {
-    const double pi = kPi;
-    const double fs = (double)p.fs;
-    const float si = __fmul_rn(p.step, __uint2float_rn(i));
-    float w = __double2float_rn(__dadd_rn(__dmul_rn(-pi, fs), (double)si));
-    w = __double2float_rn(__dadd_rn((double)w, __dmul_rn(pi, fs)));
-    const float den = __fadd_rn(w, p.w0);
-    double ph = __dmul_rn(4.0, pi);
-    ph = __dmul_rn(ph, pi);
-    ph = __dmul_rn(ph, (double)p.kdm);
-    ph = __dmul_rn(ph, (double)p.dm);
-    ph = __dmul_rn(ph, (double)w);
-    ph = __dmul_rn(ph, (double)w);
-    ph = __ddiv_rn(ph, (double)den);
-    ph = __ddiv_rn(ph, (double)p.w0);
-    ph = __ddiv_rn(ph, (double)p.w0);
-    return ph;
+    const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        const float2 x = a[i];
+        float p = x.x * x.x + x.y * x.y;
+        if (b) {
+            const float2 y = b[i];
+            p += y.x * y.x + y.y * y.y;
+        }
+        out[i] = sqrtf(p);
+    }
 }
 
-// cos/sin of a phase of up to ~1e7 rad: reduce mod 2 pi in FP64 with 2 pi
-// split into a double head and tail (Cody-Waite), then sincos.
-__device__ __forceinline__ void chirp_cis(double ph, float &c, float &s)
+// Fold n intensities (one chunk of the stream) into per-work-item partial
+// rows with the same span machinery as the fused kernel: work item w covers
+// blocks [n_blocks*w/R, n_blocks*(w+1)/R) of kFoldBlock samples.
+constexpr int kFoldBlock = 2048;
+
+__global__ void __launch_bounds__(256) fold_series_kernel(const float *__restrict__ I, long long n, int R, FoldArgs f)
 {
-    constexpr double kTwoPiHi = 6.283185307179586232;     // nearest double to 2 pi
-    constexpr double kTwoPiLo = 2.4492935982947064e-16;   // 2 pi - kTwoPiHi
-    constexpr double kInvTwoPi = 0.15915494309189533577;
-    const double n = rint(ph * kInvTwoPi);
-    double r = fma(-n, kTwoPiHi, ph);
-    r = fma(-n, kTwoPiLo, r);
-    double sd, cd;
-    sincos(r, &sd, &cd);
-    c = (float)cd;
-    s = (float)sd;
+    // trial blockIdx.y folds I[d*n ...] into partial rows w*gridDim.y + d
+    const int d = blockIdx.y, D = gridDim.y;
+    I += (size_t)d * n;
+    extern __shared__ float2 smem[];
+    float *ibuf = reinterpret_cast<float *>(smem);
+    FoldSmem fw;
+    long long *sp8 = reinterpret_cast<long long *>(ibuf + ibuf_floats(kFoldBlock));
+    fw.wa = sp8;
+    fw.wb = sp8 + f.span_cap;
+    fw.wp = reinterpret_cast<int *>(sp8 + 2 * f.span_cap);
+    fw.wd = fw.wp + f.span_cap;
+    fw.prof_main = reinterpret_cast<float *>(fw.wd + f.span_cap);
+    fw.prof_pend = fw.prof_main + f.nbins;
+    const long long nblk = (n + kFoldBlock - 1) / kFoldBlock;
+    for (int w = blockIdx.x; w < R; w += gridDim.x) {
+        const long long kb = nblk * w / R, ke = nblk * (w + 1) / R;
+        if (f.smem_prof) {
+            for (int i = threadIdx.x; i < 2 * f.nbins; i += blockDim.x)
+                fw.prof_main[i] = 0.f;
+        } else {
+            fw.prof_main = f.part_main + ((size_t)w * D + d) * f.nbins;
+            fw.prof_pend = f.part_pend + ((size_t)w * D + d) * f.nbins;
+        }
+        int sp = span_lower_bound(f.span_b, f.nspans, kb * kFoldBlock), sbase = 0, scnt = 0;
+        span_refill(f, fw, sp, sbase, scnt);
+        for (long long k = kb; k < ke; ++k) {
+            const long long t0 = k * kFoldBlock;
+            for (int t = threadIdx.x; t < kFoldBlock; t += blockDim.x)
+                ibuf[ipad(t)] = t0 + t < n ? I[t0 + t] : 0.f;
+            __syncthreads();
+            fold_block(f, fw, ibuf, t0, kFoldBlock, sp, sbase, scnt);
+            __syncthreads();
+        }
+        if (f.smem_prof) {
+            float *gm = f.part_main + ((size_t)w * D + d) * f.nbins;
+            float *gp = f.part_pend + ((size_t)w * D + d) * f.nbins;
+            for (int i = threadIdx.x; i < f.nbins; i += blockDim.x) {
+                gm[i] = fw.prof_main[i];
+                gp[i] = fw.prof_pend[i];
+            }
+        }
+        __syncthreads();
+    }
 }
+
+// ---------------------------------------------------------------------------
+// filter design on the device
+// ---------------------------------------------------------------------------
 
 template <int LOG2N, bool PP>
 __global__ void __launch_bounds__(FftShape<LOG2N>::T) design_kernel(DesignArgs a)
@@ -656,6 +689,25 @@ cudaError_t launch_fold_flush(double *am, double *ap, size_t n, cudaStream_t st)
 cudaError_t launch_fold_readout(const double *am, size_t n, double scale, float *out, cudaStream_t st)
 {
     fold_readout_kernel<<<blocks_for(n, 256), 256, 0, st>>>(am, n, scale, out);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_intensity(const float2 *a, const float2 *b, float *out, size_t n, cudaStream_t st)
+{
+    intensity_kernel<<<blocks_for(n, 256), 256, 0, st>>>(a, b, out, n);
+    return cudaGetLastError();
+}
+
+int fold_series_block() { return kFoldBlock; }
+
+cudaError_t launch_fold_series(const float *I, long long n, int R, const FoldArgs &f, int grid, int trials,
+                               cudaStream_t st)
+{
+    const size_t sm = ibuf_floats(kFoldBlock) * sizeof(float) + fold_smem_bytes(f.nbins, f.span_cap, f.smem_prof != 0);
+    cudaError_t e = set_smem(fold_series_kernel, sm);
+    if (e != cudaSuccess)
+        return e;
+    fold_series_kernel<<<dim3((unsigned)grid, (unsigned)trials), 256, sm, st>>>(I, n, R, f);
     return cudaGetLastError();
 }
 

@@ -88,5 +88,52 @@ cudaError_t launch_fold_flush(double *acc_main, double *acc_pend, size_t n, cuda
 cudaError_t launch_fold_readout(const double *acc_main, size_t n, double scale, float *out,
                                 cudaStream_t st);
 cudaError_t launch_encode_u16(const float2 *src, uint32_t *dst, size_t n, cudaStream_t st);
+// sqrt(|a|^2 + |b|^2) (b may be null)
+cudaError_t launch_intensity(const float2 *a, const float2 *b, float *out, size_t n, cudaStream_t st);
+// fold n intensities into R partial rows (fold.part_main/part_pend [R][nbins])
+int fold_series_block();
+cudaError_t launch_fold_series(const float *I, long long n, int R, const FoldArgs &f, int grid, int trials,
+                               cudaStream_t st);
+
+// ---- FFT sizes above one thread block (largefft.cu) -----------------------
+struct LargeColArgs {
+    const void *input;        // forward: the call's input (or a vector, kind 2)
+    const float2 *in;         // inverse: B[d][w][k1][n2]
+    const float2 *hist_in;    // forward windows: previous call's last M samples
+    float2 *hist_out;
+    float2 *out;              // forward: A[w][k1][n2]
+    long long N, N2, len;     // transform size, row length, vector length (kind 2)
+    int log2n, count;
+    const float2 *tw1;        // exp(sign 2 pi i e / N1) for the pass's sign
+    float2 *series;           // inverse: [d][count*M] or null
+    float *intensity;         // inverse: [d][count*M] or null
+    int detect;
+};
+struct LargeRowArgs {
+    const float2 *in;         // forward: A
+    float2 *out;              // inverse: B; design: permuted spectrum
+    float2 *ring;
+    int S;
+    long long k0;
+    int count;
+    const float2 *H;          // [d][N] permuted, x 1/N^2
+    const uint16_t *delays;   // [d][N] permuted
+    long long N;
+    int log2n;
+    const float2 *tw2;        // exp(sign 2 pi i e / N2)
+};
+void large_split(int log2n, int &log2n1, int &log2n2);
+bool large_supported(int log2n);
+cudaError_t launch_large_col_fwd(int log2n1, int kind, const LargeColArgs &a, int windows, cudaStream_t st);
+cudaError_t launch_large_col_inv(int log2n1, const LargeColArgs &a, int blocks, int trials, cudaStream_t st);
+// mode 0: forward row -> ring; 1: gather x H, inverse row -> B; 2: forward row -> out
+cudaError_t launch_large_row(int log2n2, int mode, const LargeRowArgs &a, int rows, int windows, int trials,
+                             cudaStream_t st);
+cudaError_t launch_vec_fft(int log2n, int sign, const float2 *in, float2 *out, const float2 *tw, int count,
+                           cudaStream_t st);
+cudaError_t launch_chirp_conj(const ChirpParams *cp, float2 *out, long long M, int sign, cudaStream_t st);
+cudaError_t launch_unpermute_conj(const float2 *in, float2 *out, long long K, long long K1, long long K2,
+                                  long long len_out, cudaStream_t st);
+cudaError_t launch_conj_scale(float2 *x, long long n, float scale, int conj, cudaStream_t st);
 
 }  // namespace msosm

@@ -11,6 +11,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <malloc.h>
 #include <string>
 #include <vector>
 
@@ -52,6 +53,10 @@ int usage()
 
 int main(int argc, char **argv)
 {
+    // Fold_GPU allocates folded_data_raw / tmp_fold / fold_count with new[]
+    // and accumulates into them without clearing (fold_gpu.cpp:15-18): serve
+    // every allocation from fresh zeroed pages so its sums start at zero.
+    mallopt(M_MMAP_THRESHOLD, 0);
     if (argc < 2)
         return usage();
     std::string mode = argv[1];

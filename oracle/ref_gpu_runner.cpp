@@ -14,6 +14,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <malloc.h>
 #include <string>
 #include <vector>
 
@@ -167,6 +168,10 @@ int main(int argc, char **argv)
         long tb = std::strtol(argv[9], nullptr, 10);
         if (!nd_ok(bw, dm, f0))
             return 5;
+        // Fold_GPU allocates folded_data_raw / tmp_fold / fold_count with new[]
+        // and accumulates into them without clearing (fold_gpu.cpp:15-18):
+        // serve every allocation from fresh zeroed pages so its sums start at 0.
+        mallopt(M_MMAP_THRESHOLD, 0);
         MSOSM_GPU_BATCH a(bw, dm, f0), b(bw, dm, f0);
         a.initialize_uint16(fftpoint, count);
         b.initialize_uint16(fftpoint, count);
