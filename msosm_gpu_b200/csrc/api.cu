@@ -507,6 +507,11 @@ msosm_status msosm_dedisp_create(const float *bw, const float *dm, const float *
         release(d);
         return fail(MSOSM_ERR_BAD_ARG, "count must be >= 1");
     }
+    if ((unsigned long long)count * M >= (1ull << 31)) {
+        release(d);
+        return fail(MSOSM_ERR_BAD_ARG, "count*M = %llu samples per call exceeds 2^31 - 1",
+                    (unsigned long long)count * M);
+    }
     d->M = M;
     d->N = 2 * M;
     d->log2n = log2n;
@@ -744,6 +749,8 @@ static msosm_status fold_prepare(msosm_dedisp *d, int sb, FoldArgs &fa)
     fa.part_pend = d->part_pend;
     fa.smem_prof = d->nbins <= kMaxSmemBins ? 1 : 0;
     fa.span_cap = d->win_cap;
+    fa.inv_bpt = 1.0f / (float)d->bpt;
+    fa.g_shift = fold_g_shift(d->bpt, d->large ? 256 : (int)(d->N / 16));
     return MSOSM_OK;
 }
 
@@ -984,9 +991,9 @@ msosm_status msosm_dedisp_fold_init(msosm_dedisp *d, float period, float fs, uns
         return fail(MSOSM_ERR_BAD_ARG, "period*fs gives %lu samples", ps);
     }
     const unsigned long nb = time_bin == 0 ? ps : time_bin;
-    if (nb > ps) {
+    if (nb > ps || nb > (1ul << 22)) {
         delete p;
-        return fail(MSOSM_ERR_BAD_ARG, "time_bin %lu exceeds period_samples %lu", time_bin, ps);
+        return fail(MSOSM_ERR_BAD_ARG, "time_bin %lu exceeds period_samples %lu or 2^22", nb, ps);
     }
     d->planner = p;
     d->ps = ps;
@@ -1152,8 +1159,8 @@ static void fold_release(msosm_fold *f)
 
 msosm_status msosm_fold_create(float period, float fs, unsigned long size, unsigned long time_bin, msosm_fold **out)
 {
-    if (!out || !(period > 0) || !(fs > 0) || size == 0)
-        return fail(MSOSM_ERR_BAD_ARG, "msosm_fold_create: period, fs and size must be positive");
+    if (!out || !(period > 0) || !(fs > 0) || size == 0 || size >= (1ul << 31))
+        return fail(MSOSM_ERR_BAD_ARG, "msosm_fold_create: period, fs must be positive, 0 < size < 2^31");
     *out = nullptr;
     if (msosm_device_count() == 0)
         return fail(MSOSM_ERR_NO_DEVICE, "no CUDA device");
@@ -1171,7 +1178,7 @@ msosm_status msosm_fold_create(float period, float fs, unsigned long size, unsig
         return fail(MSOSM_ERR_BAD_ARG, "period*fs gives %lu samples", f->ps);
     }
     const unsigned long nb = (time_bin == 0 || time_bin == (unsigned long)-1) ? f->ps : time_bin;
-    if (nb > f->ps) {
+    if (nb > f->ps || nb > (1ul << 22)) {
         fold_release(f);
         return fail(MSOSM_ERR_BAD_ARG, "time_bin %lu exceeds period_samples %lu", time_bin, f->ps);
     }
@@ -1354,6 +1361,8 @@ msosm_status msosm_fold_data(msosm_fold *f)
     a.part_pend = f->part_pend;
     a.smem_prof = f->nbins <= kMaxSmemBins ? 1 : 0;
     a.span_cap = f->win_cap;
+    a.inv_bpt = 1.0f / (float)f->bpt;
+    a.g_shift = fold_g_shift(f->bpt, 256);
     CK(launch_fold_series(f->I, (long long)f->size, f->R, a, f->grid, 1, f->stream));
     CK(launch_fold_reduce(f->part_main, f->part_pend, 1, f->R, f->nbins, f->acc_main, f->acc_pend, f->stream));
     // the pinned span staging is reused by the next call

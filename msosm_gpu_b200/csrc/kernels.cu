@@ -96,8 +96,7 @@ __global__ void __launch_bounds__(FftShape<LOG2N>::T) forward_kernel(FwdArgs a)
 // not depend on scheduling.
 struct FoldSmem {
     float *prof_main, *prof_pend;  // [nbins] each (or the global rows)
-    long long *wa, *wb;            // span window
-    int *wp, *wd;
+    int *wa, *wb, *wp, *wd;        // span window (chunk-local sample indices < 2^31)
 };
 
 __device__ __forceinline__ int span_lower_bound(const long long *b, int n, long long t)
@@ -119,14 +118,28 @@ __device__ __forceinline__ void span_refill(const FoldArgs &f, FoldSmem &w, int 
     __syncthreads();
     const int n = min(f.span_cap, f.nspans - at);
     for (int i = threadIdx.x; i < n; i += blockDim.x) {
-        w.wa[i] = f.span_a[at + i];
-        w.wb[i] = f.span_b[at + i];
+        w.wa[i] = (int)f.span_a[at + i];
+        w.wb[i] = (int)f.span_b[at + i];
         w.wp[i] = f.span_phase0[at + i];
         w.wd[i] = f.span_dest[at + i];
     }
     base = at;
     cnt = n;
     __syncthreads();
+}
+
+// floor(x / bpt) for x >= 0 with x / bpt < 2^22 (at most nbins + 1; the host
+// bounds nbins) from a float reciprocal, corrected to exact
+__device__ __forceinline__ int div_bpt(int x, int bpt, float inv_bpt)
+{
+    if (bpt == 1)
+        return x;
+    int q = __float2int_rz((float)x * inv_bpt);
+    if (q * bpt > x)
+        --q;
+    else if ((q + 1) * bpt <= x)
+        ++q;
+    return q;
 }
 
 // ibuf holds intensities at index t + t/32 (one pad slot per 32 samples), so
@@ -137,28 +150,27 @@ __device__ __forceinline__ void fold_piece(const FoldArgs &f, float *prof, const
                                            int ph_lo, int ph_hi)
 {
     // sample of phase p sits at chunk-local block offset off + p.  Each bin is
-    // summed by a group of G lanes (G ~ bpt/8, a power of two <= 32), lane l
-    // taking samples l, l+G, ...; the group then reduces with a fixed xor
-    // butterfly.  G*bins ~ M/8 keeps every warp of the block busy for any bin
-    // length, and the loop trip count is uniform so whole warps shuffle.
-    const int b_lo = ph_lo / f.bpt;
-    int b_hi = (ph_hi - 1) / f.bpt;
+    // summed by a group of G = 2^g_shift lanes (G ~ bpt/8, a power of two <= 32,
+    // chosen on the host), lane l taking samples l, l+G, ...; the group then
+    // reduces with a fixed xor butterfly.  G*bins ~ M/8 keeps every warp of
+    // the block busy for any bin length, and the loop trip count is uniform
+    // so whole warps shuffle.
+    const int b_lo = div_bpt(ph_lo, f.bpt, f.inv_bpt);
+    int b_hi = div_bpt(ph_hi - 1, f.bpt, f.inv_bpt);
     if (b_hi > f.nbins - 1)
         b_hi = f.nbins - 1;
     if (b_hi < b_lo)
         return;
-    int G = 1;
-    while (G < 32 && G * 8 < f.bpt)
-        G <<= 1;
-    if ((int)blockDim.x < 32)
-        G = 1;  // tiny FFTs: blocks of fewer than 32 threads
-    const int g = threadIdx.x / G, l = threadIdx.x % G, ngroups = blockDim.x / G;
+    const int G = 1 << f.g_shift;
+    const int g = (int)threadIdx.x >> f.g_shift, l = (int)threadIdx.x & (G - 1);
+    const int ngroups = (int)blockDim.x >> f.g_shift;
     for (int first = b_lo; first <= b_hi; first += ngroups) {
         const int bin = first + g;
         float a0 = 0.f, a1 = 0.f;
         if (bin <= b_hi) {
-            const int s_lo = max(ph_lo, bin * f.bpt);
-            const int s_hi = min(ph_hi, (bin + 1) * f.bpt);
+            const int s0 = bin * f.bpt;
+            const int s_lo = max(ph_lo, s0);
+            const int s_hi = min(ph_hi, s0 + f.bpt);
             int p = s_lo + l;
             for (; p + G < s_hi; p += 2 * G) {
                 a0 += ibuf[ipad(off + p)];
@@ -177,7 +189,7 @@ __device__ __forceinline__ void fold_piece(const FoldArgs &f, float *prof, const
 
 // Fold the M intensities of one block (ibuf: chunk-local samples t0..t0+M-1).
 // sp/base/cnt: the work item's running span cursor and window (uniform).
-__device__ __forceinline__ void fold_block(const FoldArgs &f, FoldSmem &w, const float *ibuf, long long t0, int M,
+__device__ __forceinline__ void fold_block(const FoldArgs &f, FoldSmem &w, const float *ibuf, int t0, int M,
                                            int &sp, int &base, int &cnt)
 {
     // advance to the first span ending after t0
@@ -189,25 +201,24 @@ __device__ __forceinline__ void fold_block(const FoldArgs &f, FoldSmem &w, const
         else
             break;
     }
+    const int t1 = t0 + M;
     for (int s = sp; s < f.nspans; ++s) {
         if (s >= base + cnt)
             span_refill(f, w, s, base, cnt);
         const int i = s - base;
-        const long long sa = w.wa[i];
-        if (sa >= t0 + M)
+        const int sa = w.wa[i];
+        if (sa >= t1)
             break;
         const int dest = w.wd[i];
         if (dest != 0) {
-            const long long a = sa > t0 ? sa : t0;
-            const long long sb = w.wb[i];
-            const long long b = sb < t0 + M ? sb : t0 + M;
+            const int sb = w.wb[i];
+            const int a = max(sa, t0), b = min(sb, t1);
             if (a < b) {
-                const int ph_lo = w.wp[i] + (int)(a - sa);
-                const int ph_hi = ph_lo + (int)(b - a);
-                fold_piece(f, dest == 1 ? w.prof_main : w.prof_pend, ibuf, (int)(a - t0) - ph_lo, ph_lo, ph_hi);
+                const int ph_lo = w.wp[i] + (a - sa);
+                fold_piece(f, dest == 1 ? w.prof_main : w.prof_pend, ibuf, a - t0 - ph_lo, ph_lo, ph_lo + (b - a));
             }
             // a later span of this block may fold into the same bins
-            if (w.wb[i] < t0 + M)
+            if (sb < t1)
                 __syncthreads();
         }
     }
@@ -225,11 +236,10 @@ __global__ void __launch_bounds__(FftShape<LOG2N>::T) dedisp_kernel(DedispArgs a
     float *ibuf = reinterpret_cast<float *>(smem + (PP ? 2 : 1) * F::SMEM);
     FoldSmem fw;
     if constexpr (FOLD) {
-        // after ibuf: [span window a, b (8-byte)] [phase0, dest] [prof_main, prof_pend]
-        long long *sp8 = reinterpret_cast<long long *>(ibuf + ibuf_floats(M));
-        fw.wa = sp8;
-        fw.wb = sp8 + a.fold.span_cap;
-        fw.wp = reinterpret_cast<int *>(sp8 + 2 * a.fold.span_cap);
+        // after ibuf: [span window a, b, phase0, dest] [prof_main, prof_pend]
+        fw.wa = reinterpret_cast<int *>(ibuf + ibuf_floats(M));
+        fw.wb = fw.wa + a.fold.span_cap;
+        fw.wp = fw.wb + a.fold.span_cap;
         fw.wd = fw.wp + a.fold.span_cap;
         fw.prof_main = reinterpret_cast<float *>(fw.wd + a.fold.span_cap);
         fw.prof_pend = fw.prof_main + a.fold.nbins;
@@ -302,7 +312,7 @@ __global__ void __launch_bounds__(FftShape<LOG2N>::T) dedisp_kernel(DedispArgs a
             }
             if constexpr (FOLD) {
                 __syncthreads();
-                fold_block(a.fold, fw, ibuf, (long long)k * M, M, sp, sbase, scnt);
+                fold_block(a.fold, fw, ibuf, k * M, M, sp, sbase, scnt);
             }
         }
         if constexpr (FOLD) {
@@ -353,10 +363,9 @@ __global__ void __launch_bounds__(256) fold_series_kernel(const float *__restric
     extern __shared__ float2 smem[];
     float *ibuf = reinterpret_cast<float *>(smem);
     FoldSmem fw;
-    long long *sp8 = reinterpret_cast<long long *>(ibuf + ibuf_floats(kFoldBlock));
-    fw.wa = sp8;
-    fw.wb = sp8 + f.span_cap;
-    fw.wp = reinterpret_cast<int *>(sp8 + 2 * f.span_cap);
+    fw.wa = reinterpret_cast<int *>(ibuf + ibuf_floats(kFoldBlock));
+    fw.wb = fw.wa + f.span_cap;
+    fw.wp = fw.wb + f.span_cap;
     fw.wd = fw.wp + f.span_cap;
     fw.prof_main = reinterpret_cast<float *>(fw.wd + f.span_cap);
     fw.prof_pend = fw.prof_main + f.nbins;
@@ -373,9 +382,9 @@ __global__ void __launch_bounds__(256) fold_series_kernel(const float *__restric
         int sp = span_lower_bound(f.span_b, f.nspans, kb * kFoldBlock), sbase = 0, scnt = 0;
         span_refill(f, fw, sp, sbase, scnt);
         for (long long k = kb; k < ke; ++k) {
-            const long long t0 = k * kFoldBlock;
+            const int t0 = (int)(k * kFoldBlock);
             for (int t = threadIdx.x; t < kFoldBlock; t += blockDim.x)
-                ibuf[ipad(t)] = t0 + t < n ? I[t0 + t] : 0.f;
+                ibuf[ipad(t)] = (long long)t0 + t < n ? I[t0 + t] : 0.f;
             __syncthreads();
             fold_block(f, fw, ibuf, t0, kFoldBlock, sp, sbase, scnt);
             __syncthreads();
@@ -555,7 +564,7 @@ static cudaError_t forward_t(InputKind kind, const FwdArgs &a, cudaStream_t st)
 
 size_t fold_smem_bytes(int nbins, int span_cap, bool smem_prof)
 {
-    return (size_t)span_cap * (2 * sizeof(long long) + 2 * sizeof(int)) +
+    return (size_t)span_cap * 4 * sizeof(int) +
            (smem_prof ? 2 * (size_t)nbins * sizeof(float) : 0);
 }
 

@@ -34,7 +34,20 @@ struct FoldArgs {
     float *part_main, *part_pend;  // [items][nbins]
     int smem_prof;  // 1: the work item's profile rows live in shared memory
     int span_cap;   // spans held in the shared-memory window (>= spans one block can touch)
+    float inv_bpt;  // 1/bpt, for the exact-corrected division
+    int g_shift;    // log2 of the lanes summing one bin (fold_g_shift)
 };
+
+// Lanes per bin in the fold: G ~ bpt/8, a power of two <= 32 (1 below whole warps).
+inline int fold_g_shift(int bpt, int threads)
+{
+    if (threads < 32)
+        return 0;
+    int g = 0;
+    while (g < 5 && (8 << g) < bpt)
+        ++g;
+    return g;
+}
 
 // intensity staging of one block: M samples, one pad slot per 32
 __host__ __device__ constexpr int ibuf_floats(int m) { return (m + (m >> 5) + 1) & ~1; }
