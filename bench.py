@@ -224,7 +224,7 @@ def run_ours(args):
     # ---- value: input resident in HBM, one call per step -----------------
     blocks = samples // (FFTPOINT // 2)
     stream = torch.cuda.Stream(dev)
-    d = Dedisperser(BW, dms, F0, FFTPOINT, count=blocks, series=False)
+    d = Dedisperser(BW, dms, F0, FFTPOINT, count=blocks, series=False, precision=args.precision)
     d.set_stream(stream)
     nd_max = int(d.Nd.max())
     d.fold_init(PULSAR["period"], BW, time_bin=NBINS, discard_Nd=nd_max, detect="power")
@@ -264,7 +264,7 @@ def run_ours(args):
     # ---- e2e: pinned host input through the C ABI, chunked calls -----------
     e_count = min(blocks, 4096)
     calls = blocks // e_count
-    de = Dedisperser(BW, dms, F0, FFTPOINT, count=e_count, series=False)
+    de = Dedisperser(BW, dms, F0, FFTPOINT, count=e_count, series=False, precision=args.precision)
     de.fold_init(PULSAR["period"], BW, time_bin=NBINS, discard_Nd=nd_max, detect="power")
     xh = torch.from_numpy(x).pin_memory().numpy()
     chunk = e_count * (FFTPOINT // 2)
@@ -413,6 +413,8 @@ def main():
     ap.add_argument("--log2-samples", type=int, default=LOG2_SAMPLES)
     ap.add_argument("--dms", type=int, default=N_DM)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp16"],
+                    help="inverse transforms on the CUDA cores (fp32) or the tensor cores (fp16)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -123,6 +123,12 @@ typedef struct msosm_dedisp msosm_dedisp;
 /* flags for msosm_dedisp_create */
 #define MSOSM_FLAG_OSM 0x1u      /* classical overlap-save (OSM_GPU_*) instead of MS-OSM */
 #define MSOSM_FLAG_NO_SERIES 0x2u /* do not materialise the dedispersed series (fold only) */
+/* Inverse transforms on the tensor cores: f16 operands with a per-block
+ * power-of-two scale, f32 accumulation.  No counterpart in the reference
+ * (its inverse transform is the FP32 cuFFT).  FFT size 4096 only (other
+ * sizes return MSOSM_ERR_UNSUPPORTED).  Relative RMS error of the series
+ * against FP64: about 5e-4; folded profiles much lower. */
+#define MSOSM_FLAG_TENSOR_F16 0x4u
 
 typedef struct msosm_dedisp_info {
     unsigned long M;        /* hop / filter order; FFT size is 2M */
@@ -277,6 +283,19 @@ MSOSM_API msosm_status msosm_fold_planner_create(float period, float fs, unsigne
 MSOSM_API msosm_status msosm_fold_planner_destroy(msosm_fold_planner *p);
 MSOSM_API msosm_status msosm_fold_planner_chunk(msosm_fold_planner *p, unsigned long size, int64_t *dest,
                                       unsigned long long *completed);
+
+/* ======================================================================
+ * Diagnostics (no counterpart in the reference)
+ * ====================================================================== */
+
+/* Runs one of the two tensor-core GEMMs of MSOSM_FLAG_TENSOR_F16 on given
+ * data, with the kernel's own shared-memory layouts, constant operand and
+ * tensor-memory read-back: d = a * B_step, where a is a 128 x 128 matrix of
+ * f16 bit patterns (row-major, host memory) and B_step the real form of the
+ * 64-point inverse DFT (step 1: 128 x 128, outputs [Re | Im] of all 64
+ * frequencies; step 2: 128 x 64, outputs [Re | Im] of frequencies 32..63).
+ * d: host, 128 x (step 1 ? 128 : 64) floats, row-major.  Needs a GPU. */
+MSOSM_API msosm_status msosm_tc_gemm_check(int step, const uint16_t *a, float *d);
 
 #ifdef __cplusplus
 }

@@ -24,6 +24,7 @@ ERR_NO_DEVICE = 7
 
 FLAG_OSM = 0x1
 FLAG_NO_SERIES = 0x2
+FLAG_TENSOR_F16 = 0x4
 DETECT_POWER = 0
 DETECT_AMPLITUDE = 1
 
@@ -109,6 +110,7 @@ def _declare(L: ctypes.CDLL) -> None:
         "msosm_fold_planner_create": (i32, [f32, f32, ul, pvp]),
         "msosm_fold_planner_destroy": (i32, [vp]),
         "msosm_fold_planner_chunk": (i32, [vp, ul, vp, pull]),
+        "msosm_tc_gemm_check": (i32, [i32, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -1,6 +1,7 @@
 // api.cu -- the C ABI (include/msosm_b200.h) over the sm_100a kernels.
 #include "msosm_b200.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -14,6 +15,7 @@
 
 #include "host_prepare.hpp"
 #include "kernels.hpp"
+#include "tc_layout.hpp"
 
 using namespace msosm;
 
@@ -128,6 +130,14 @@ struct msosm_dedisp {
     int *span_p_d = nullptr, *span_dest_d = nullptr;
     // pinned span staging: [2][cap] of a, b, phase0, dest
     long long *span_host = nullptr;
+    // inverse transforms on the tensor cores (MSOSM_FLAG_TENSOR_F16): ring,
+    // H and delays in tensor-core order (tc_layout.hpp); status_d != 0 after
+    // a timed-out wait in the kernel
+    bool tc = false;
+    int *status_d = nullptr;
+    float *row_max = nullptr;  // [S] largest |component| of each ring row
+    float *h_max = nullptr;    // [D] largest |component| of each trial's H
+    int *delay_max_d = nullptr; // [D] largest block delay of each trial
     // FFT above one thread block: four-step N = N1*N2, spectra in [k1][k2] order
     bool large = false;
     int log2n1 = 0, log2n2 = 0;
@@ -158,7 +168,8 @@ void release(msosm_dedisp *d)
     void *bufs[] = {d->ring, d->H, d->hist, d->series_buf, d->delays_d, d->tw_fwd, d->tw_inv, d->tw_inv_m,
                     d->staging[0], d->staging[1], d->u16_out, d->part_main, d->part_pend, d->prof_out,
                     d->acc_main, d->acc_pend, d->span_a_d, d->span_b_d, d->span_p_d, d->span_dest_d,
-                    d->lA, d->lB, d->lI, d->tw1f, d->tw1i, d->tw2f, d->tw2i};
+                    d->lA, d->lB, d->lI, d->tw1f, d->tw1i, d->tw2f, d->tw2i, d->status_d,
+                    d->row_max, d->h_max, d->delay_max_d};
     for (void *p : bufs)
         if (p)
             cudaFree(p);
@@ -229,19 +240,25 @@ cudaError_t plan_grid(msosm_dedisp *d)
     if (e != cudaSuccess)
         return e;
     const size_t extra = d->fold ? fold_smem_bytes(d->nbins, d->win_cap, d->nbins <= kMaxSmemBins) : 0;
-    int per_sm = dedisp_blocks_per_sm(d->log2n, d->pingpong, d->series, d->fold, extra);
+    int per_sm = d->tc ? tc_blocks_per_sm(d->series, d->fold, extra)
+                       : dedisp_blocks_per_sm(d->log2n, d->pingpong, d->series, d->fold, extra);
     if (per_sm < 1)
         per_sm = 1;
     const long long resident = (long long)per_sm * sms;
     long long R = (8 * resident + d->D - 1) / d->D;
-    if (R > d->count)
-        R = d->count;
+    // the tensor-core kernel works on pairs of blocks
+    const long long units = d->tc ? (d->count + 1) / 2 : d->count;
+    if (R > units)
+        R = units;
     if (R < 1)
         R = 1;
     d->R = (int)R;
     const long long items = (long long)d->D * R;
     const long long waves = (items + resident - 1) / resident;
     d->grid = (int)((items + waves - 1) / waves);
+    if (std::getenv("MSOSM_DEBUG_GRID"))
+        std::fprintf(stderr, "msosm plan_grid: tc=%d fold=%d series=%d extra=%zu per_sm=%d R=%d grid=%d\n",
+                     (int)d->tc, (int)d->fold, (int)d->series, extra, per_sm, d->R, d->grid);
     return cudaSuccess;
 }
 
@@ -462,7 +479,7 @@ msosm_status msosm_dedisp_create(const float *bw, const float *dm, const float *
     if (!out || !bw || !dm || !f0 || numDMs < 1)
         return fail(MSOSM_ERR_BAD_ARG, "msosm_dedisp_create: null argument or numDMs < 1");
     *out = nullptr;
-    if (flags & ~(MSOSM_FLAG_OSM | MSOSM_FLAG_NO_SERIES))
+    if (flags & ~(MSOSM_FLAG_OSM | MSOSM_FLAG_NO_SERIES | MSOSM_FLAG_TENSOR_F16))
         return fail(MSOSM_ERR_BAD_ARG, "unknown flags 0x%x", flags);
     for (int i = 0; i < numDMs; ++i)
         if (!(bw[i] > 0) || !(f0[i] > 0) || !(dm[i] >= 0) || !std::isfinite(dm[i]))
@@ -501,6 +518,11 @@ msosm_status msosm_dedisp_create(const float *bw, const float *dm, const float *
         return fail(MSOSM_ERR_UNSUPPORTED, "FFT size %lu outside the supported 64..2^24", 2 * M);
     }
     d->large = !log2n_supported(log2n);
+    d->tc = (flags & MSOSM_FLAG_TENSOR_F16) != 0;
+    if (d->tc && !tc_supported(log2n)) {
+        release(d);
+        return fail(MSOSM_ERR_UNSUPPORTED, "MSOSM_FLAG_TENSOR_F16 needs FFT size %d (got %lu)", tc::kN, 2 * M);
+    }
     if (input_size != 0)
         count = (int)(input_size / M);
     if (count < 1) {
@@ -582,13 +604,15 @@ msosm_status msosm_dedisp_create(const float *bw, const float *dm, const float *
         large_split(log2n, d->log2n1, d->log2n2);
     {
         // per-bin delays on the device; for the four-step layout permuted to
-        // position k1*N2 + k2 of bin k1 + N1*k2
+        // position k1*N2 + k2 of bin k1 + N1*k2, for the tensor-core kernel
+        // to tc_pos(bin)
         std::vector<uint16_t> dl(d->delays.size());
         const unsigned long N1 = 1ul << d->log2n1, N2 = 1ul << d->log2n2;
         for (int t = 0; t < numDMs; ++t)
             for (unsigned long p = 0; p < N; ++p) {
                 const unsigned long b = d->large ? (p / N2) + N1 * (p % N2) : p;
-                dl[(size_t)t * N + p] = (uint16_t)d->delays[(size_t)t * N + b];
+                const unsigned long q = d->tc ? (unsigned long)tc::tc_pos((int)p) : p;
+                dl[(size_t)t * N + q] = (uint16_t)d->delays[(size_t)t * N + b];
             }
         CKD(cudaMemcpy(d->delays_d, dl.data(), sizeof(uint16_t) * dl.size(), cudaMemcpyHostToDevice));
     }
@@ -608,6 +632,37 @@ msosm_status msosm_dedisp_create(const float *bw, const float *dm, const float *
         if ((s = design_filters(log2n, cp, scale, -1, d->tw_inv_m, d->tw_fwd, d->H, d->stream)) != MSOSM_OK) {
             release(d);
             return s;
+        }
+        if (d->tc) {
+            float2 *tmp = nullptr;
+            CKD(cudaMalloc((void **)&tmp, sizeof(float2) * (size_t)numDMs * N));
+            cudaError_t e = launch_tc_permute_rows(d->H, tmp, numDMs, d->stream);
+            if (e == cudaSuccess)
+                e = cudaMemcpyAsync(d->H, tmp, sizeof(float2) * (size_t)numDMs * N, cudaMemcpyDeviceToDevice,
+                                    d->stream);
+            if (e == cudaSuccess)
+                e = cudaStreamSynchronize(d->stream);
+            cudaFree(tmp);
+            CKD(e);
+            CKD(dalloc(&d->status_d, 1, tot));
+            CKD(cudaMemset(d->status_d, 0, sizeof(int)));
+            // scale bounds: ring rows not yet written hold zero
+            CKD(dalloc(&d->row_max, (size_t)d->S, tot));
+            CKD(cudaMemset(d->row_max, 0, sizeof(float) * d->S));
+            std::vector<float2> hh((size_t)numDMs * N);
+            CKD(cudaMemcpy(hh.data(), d->H, sizeof(float2) * hh.size(), cudaMemcpyDeviceToHost));
+            std::vector<float> hm(numDMs, 0.f);
+            std::vector<int> dmx(numDMs, 0);
+            for (int t = 0; t < numDMs; ++t)
+                for (unsigned long b = 0; b < N; ++b) {
+                    const float2 v = hh[(size_t)t * N + b];
+                    hm[t] = std::fmax(hm[t], std::fmax(std::fabs(v.x), std::fabs(v.y)));
+                    dmx[t] = std::max(dmx[t], d->delays[(size_t)t * N + b]);
+                }
+            CKD(dalloc(&d->h_max, (size_t)numDMs, tot));
+            CKD(dalloc(&d->delay_max_d, (size_t)numDMs, tot));
+            CKD(cudaMemcpy(d->h_max, hm.data(), sizeof(float) * numDMs, cudaMemcpyHostToDevice));
+            CKD(cudaMemcpy(d->delay_max_d, dmx.data(), sizeof(int) * numDMs, cudaMemcpyHostToDevice));
         }
         CKD(plan_grid(d));
     } else {
@@ -690,7 +745,7 @@ msosm_status msosm_dedisp_get_dedisp_params(const msosm_dedisp *d, int i, msosm_
     const unsigned long N1 = 1ul << d->log2n1, N2 = 1ul << d->log2n2;
     for (unsigned long b = 0; b < d->N; ++b) {
         // four-step layout: bin b = k1 + N1*k2 sits at k1*N2 + k2
-        const unsigned long p = d->large ? (b % N1) * N2 + b / N1 : b;
+        const unsigned long p = d->large ? (b % N1) * N2 + b / N1 : (d->tc ? (unsigned long)tc::tc_pos((int)b) : b);
         H[b].x = tmp[p].x * up;
         H[b].y = tmp[p].y * up;
     }
@@ -832,6 +887,19 @@ static msosm_status filter_block_large(msosm_dedisp *d, const void *src, InputKi
     return MSOSM_OK;
 }
 
+// After the handle's stream has drained: a timed-out wait of the
+// tensor-core kernel (its results are then invalid).
+static msosm_status kernel_status(msosm_dedisp *d)
+{
+    if (!d->status_d)
+        return MSOSM_OK;
+    int st = 0;
+    CK(cudaMemcpy(&st, d->status_d, sizeof(int), cudaMemcpyDeviceToHost));
+    if (st != 0)
+        return fail(MSOSM_ERR_TIMEOUT, "tensor-core kernel: a wait on the tensor core timed out");
+    return MSOSM_OK;
+}
+
 static msosm_status filter_block(msosm_dedisp *d, const void *input, InputKind kind)
 {
     if (check_handle(d) || !input)
@@ -868,7 +936,7 @@ static msosm_status filter_block(msosm_dedisp *d, const void *input, InputKind k
     }
     if (d->large)
         return filter_block_large(d, src, kind, ev, launches0);
-    FwdArgs fa;
+    FwdArgs fa{};
     fa.input = src;
     fa.hist_in = d->hist + (size_t)(d->calls & 1) * d->M;
     fa.hist_out = d->hist + (size_t)((d->calls + 1) & 1) * d->M;
@@ -877,6 +945,8 @@ static msosm_status filter_block(msosm_dedisp *d, const void *input, InputKind k
     fa.k0 = (long long)d->calls * d->count;
     fa.count = d->count;
     fa.tw = d->tw_fwd;
+    fa.tc_order = d->tc ? 1 : 0;
+    fa.row_max = d->row_max;
     if (ev)
         CK(cudaEventRecord(ev->e[0], d->stream));
     CK(launch_forward(d->log2n, kind, fa, d->stream));
@@ -885,7 +955,7 @@ static msosm_status filter_block(msosm_dedisp *d, const void *input, InputKind k
     if (ev)
         CK(cudaEventRecord(ev->e[1], d->stream));
 
-    DedispArgs da;
+    DedispArgs da{};
     da.ring = d->ring;
     da.S = d->S;
     da.max_delay = d->max_delay;
@@ -898,6 +968,10 @@ static msosm_status filter_block(msosm_dedisp *d, const void *input, InputKind k
     da.tw = d->tw_inv;
     da.series = d->series_buf;
     da.fold.nspans = -1;
+    da.status = d->status_d;
+    da.row_max = d->row_max;
+    da.h_max = d->h_max;
+    da.delay_max = d->delay_max_d;
     if (d->fold) {
         msosm_status st = fold_prepare(d, sb, da.fold);
         if (st != MSOSM_OK)
@@ -907,7 +981,10 @@ static msosm_status filter_block(msosm_dedisp *d, const void *input, InputKind k
     // the dedispersion kernel is timed alone
     if (ev)
         CK(cudaEventRecord(ev->e[2], d->stream));
-    CK(launch_dedisp(d->log2n, d->pingpong, d->series, d->fold, da, d->grid, d->stream));
+    if (d->tc)
+        CK(launch_tc_dedisp(d->series, d->fold, da, d->grid, d->stream));
+    else
+        CK(launch_dedisp(d->log2n, d->pingpong, d->series, d->fold, da, d->grid, d->stream));
     d->launches += 1;
     if (ev)
         CK(cudaEventRecord(ev->e[3], d->stream));
@@ -945,7 +1022,7 @@ msosm_status msosm_dedisp_get_output_c64(msosm_dedisp *d, msosm_complex *out)
     const size_t n = (size_t)d->D * d->count * d->M + 1;
     CK(cudaMemcpyAsync(out, d->series_buf, sizeof(float2) * n, cudaMemcpyDeviceToHost, d->stream));
     CK(cudaStreamSynchronize(d->stream));
-    return MSOSM_OK;
+    return kernel_status(d);
 }
 
 msosm_status msosm_dedisp_get_output_uint16(msosm_dedisp *d, msosm_uint16_pair *out)
@@ -960,7 +1037,7 @@ msosm_status msosm_dedisp_get_output_uint16(msosm_dedisp *d, msosm_uint16_pair *
     CK(launch_encode_u16(d->series_buf, d->u16_out, n, d->stream));
     CK(cudaMemcpyAsync(out, d->u16_out, sizeof(uint32_t) * n, cudaMemcpyDeviceToHost, d->stream));
     CK(cudaStreamSynchronize(d->stream));
-    return MSOSM_OK;
+    return kernel_status(d);
 }
 
 msosm_status msosm_dedisp_output_device_ptr(msosm_dedisp *d, msosm_complex **ptr)
@@ -1058,7 +1135,7 @@ msosm_status msosm_dedisp_get_profiles(msosm_dedisp *d, float *out)
     CK(launch_fold_readout(d->acc_main, n, d->out_scale, d->prof_out, d->stream));
     CK(cudaMemcpyAsync(out, d->prof_out, sizeof(float) * n, cudaMemcpyDeviceToHost, d->stream));
     CK(cudaStreamSynchronize(d->stream));
-    return MSOSM_OK;
+    return kernel_status(d);
 }
 
 msosm_status msosm_dedisp_folded_periods(const msosm_dedisp *d, unsigned long long *n)
@@ -1075,7 +1152,7 @@ msosm_status msosm_dedisp_synchronize(msosm_dedisp *d)
         return MSOSM_ERR_BAD_ARG;
     CK(cudaStreamSynchronize(d->stream));
     CK(cudaStreamSynchronize(d->copy_stream));
-    return MSOSM_OK;
+    return kernel_status(d);
 }
 
 msosm_status msosm_dedisp_enable_timing(msosm_dedisp *d, int on)
@@ -1437,6 +1514,44 @@ msosm_status msosm_fold_planner_chunk(msosm_fold_planner *p, unsigned long size,
     }
     if (completed)
         *completed = p->p.completed_folded();
+    return MSOSM_OK;
+}
+
+msosm_status msosm_tc_gemm_check(int step, const uint16_t *a, float *d)
+{
+    if ((step != 1 && step != 2) || !a || !d)
+        return fail(MSOSM_ERR_BAD_ARG, "step must be 1 or 2; a and d non-null");
+    if (msosm_device_count() == 0)
+        return fail(MSOSM_ERR_NO_DEVICE, "no CUDA device");
+    const size_t na = 128 * 128, nd = (size_t)128 * (step == 1 ? 128 : 64);
+    uint16_t *ad = nullptr;
+    float *dd = nullptr;
+    int *st = nullptr;
+    int status = 0;
+    cudaError_t e = cudaMalloc((void **)&ad, sizeof(uint16_t) * na);
+    if (e == cudaSuccess)
+        e = cudaMalloc((void **)&dd, sizeof(float) * nd);
+    if (e == cudaSuccess)
+        e = cudaMalloc((void **)&st, sizeof(int));
+    if (e == cudaSuccess)
+        e = cudaMemset(st, 0, sizeof(int));
+    if (e == cudaSuccess)
+        e = cudaMemcpy(ad, a, sizeof(uint16_t) * na, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+        e = launch_tc_probe(step, ad, dd, st, nullptr);
+    if (e == cudaSuccess)
+        e = cudaDeviceSynchronize();
+    if (e == cudaSuccess)
+        e = cudaMemcpy(d, dd, sizeof(float) * nd, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess)
+        e = cudaMemcpy(&status, st, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(ad);
+    cudaFree(dd);
+    cudaFree(st);
+    if (e != cudaSuccess)
+        return cuda_fail(e, "tensor-core GEMM check");
+    if (status != 0)
+        return fail(MSOSM_ERR_TIMEOUT, "tensor-core GEMM check: wait timed out");
     return MSOSM_OK;
 }
 

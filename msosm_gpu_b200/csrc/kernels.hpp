@@ -22,6 +22,8 @@ struct FwdArgs {
     long long k0;           // global index of this call's first block
     int count;
     const float2 *tw;       // exp(-2 pi i e/N)
+    int tc_order;           // 1: rows in tensor-core order (4096-point only)
+    float *row_max;         // tc_order: [S] largest |component| of each ring row
 };
 
 struct FoldArgs {
@@ -69,6 +71,11 @@ struct DedispArgs {
     const float2 *tw;         // exp(+2 pi i e/N)
     float2 *series;           // [D][count*M] or nullptr
     FoldArgs fold;            // fold.nspans < 0: no folding
+    // tensor-core kernel only
+    int *status;              // nonzero after a timed-out wait
+    const float *row_max;     // [S] largest |component| of each ring row
+    const float *h_max;       // [D] largest |component| of each trial's H
+    const int *delay_max;     // [D] largest block delay of each trial
 };
 
 struct DesignArgs {
@@ -107,6 +114,20 @@ cudaError_t launch_intensity(const float2 *a, const float2 *b, float *out, size_
 int fold_series_block();
 cudaError_t launch_fold_series(const float *I, long long n, int R, const FoldArgs &f, int grid, int trials,
                                cudaStream_t st);
+
+// ---- tensor-core (tcgen05) dedispersion, 4096-point transforms (tc_dedisp.cu)
+bool tc_supported(int log2n);
+// dynamic shared memory of the tensor-core kernel with `extra` fold bytes
+size_t tc_smem_bytes(size_t extra);
+int tc_blocks_per_sm(bool series, bool fold, size_t extra_smem);
+// a.H and a.delays in tensor-core order (tc_layout.hpp), ring written with
+// FwdArgs::tc_order; a.R counts ranges of block pairs
+cudaError_t launch_tc_dedisp(bool series, bool fold, const DedispArgs &a, int grid, cudaStream_t st);
+// rows of n bins (n = 4096) from natural into tensor-core order, in place via scratch
+cudaError_t launch_tc_permute_rows(const float2 *in, float2 *out, int rows, cudaStream_t st);
+// one GEMM of the kernel on given data: a = 128 x 128 f16 bit patterns
+// (row-major, M x K), d = 128 x (step 1 ? 128 : 64) f32 (row-major)
+cudaError_t launch_tc_probe(int step, const uint16_t *a, float *d, int *status, cudaStream_t st);
 
 // ---- FFT sizes above one thread block (largefft.cu) -----------------------
 struct LargeColArgs {

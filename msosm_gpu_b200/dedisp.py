@@ -69,11 +69,15 @@ class Dedisperser:
     dm: trial DMs.  fftpoint 0 picks the minimum; a smaller one is raised to
     the minimum like the reference does.  ``series`` materialises the
     dedispersed series (needed by get_output); ``osm`` selects classical
-    overlap-save.
+    overlap-save.  ``precision`` "fp32" (default) runs the inverse transforms
+    on the CUDA cores in FP32; "fp16" runs them on the tensor cores with f16
+    operands and f32 accumulation (FFT size 4096 only).
     """
 
     def __init__(self, bw, dm, f0, fftpoint: int = 0, count: int = 1, input_size: int = 0,
-                 osm: bool = False, series: bool = True):
+                 osm: bool = False, series: bool = True, precision: str = "fp32"):
+        if precision not in ("fp32", "fp16"):
+            raise ValueError("precision must be 'fp32' or 'fp16'")
         dm = _f32_array(dm)
         n = dm.size
         bw = _f32_array(bw, n)
@@ -81,7 +85,8 @@ class Dedisperser:
         if bw.size != n or f0.size != n:
             raise ValueError("bw, dm, f0 must be scalars or arrays of one length")
         self._params = (bw, dm, f0)
-        flags = (_abi.FLAG_OSM if osm else 0) | (0 if series else _abi.FLAG_NO_SERIES)
+        flags = ((_abi.FLAG_OSM if osm else 0) | (0 if series else _abi.FLAG_NO_SERIES)
+                 | (_abi.FLAG_TENSOR_F16 if precision == "fp16" else 0))
         h = ctypes.c_void_p()
         check(lib().msosm_dedisp_create(bw.ctypes.data, dm.ctypes.data, f0.ctypes.data, n,
                                         int(fftpoint), int(count), int(input_size), flags,
@@ -96,6 +101,7 @@ class Dedisperser:
         self.ring_slots = int(info.ring_slots)
         self.osm = osm
         self.series = series
+        self.precision = precision
         nd = np.zeros(n, np.uint64)
         check(lib().msosm_dedisp_get_nd(self._h, nd.ctypes.data))
         self.Nd = nd
@@ -315,3 +321,15 @@ class OSM_GPU_DM_concurrent(MSOSM_GPU_DM_concurrent):
         self.M_common_min = self._d.M_min
         self.Nd = self._d.Nd
         self.compute_only = compute_only
+
+
+def tc_gemm_check(step: int, a: np.ndarray) -> np.ndarray:
+    """Run GEMM ``step`` (1 or 2) of the tensor-core kernel on a 128 x 128
+    float16 matrix ``a`` with the kernel's own layouts (msosm_tc_gemm_check);
+    returns a @ B_step as float32 (128 x 128 for step 1, 128 x 64 for step 2)."""
+    a = np.ascontiguousarray(a, dtype=np.float16)
+    if a.shape != (128, 128):
+        raise ValueError("a must be 128 x 128")
+    d = np.zeros((128, 128 if step == 1 else 64), np.float32)
+    check(lib().msosm_tc_gemm_check(int(step), a.view(np.uint16).ctypes.data, d.ctypes.data))
+    return d

@@ -45,6 +45,49 @@ def test_no_device_is_reported_not_crashed():
     assert st == _abi.ERR_NO_DEVICE and not h.value
 
 
+def test_tensor_path_rejects_other_fft_sizes():
+    # checked before any device work, so this holds with or without a GPU
+    bw = np.array([16e6], np.float32)
+    dm = np.array([5.0], np.float32)
+    f0 = np.array([1242e6], np.float32)
+    h = ctypes.c_void_p()
+    st = _abi.lib().msosm_dedisp_create(bw.ctypes.data, dm.ctypes.data, f0.ctypes.data, 1, 2048, 4, 0,
+                                        _abi.FLAG_TENSOR_F16, ctypes.byref(h))
+    assert st == _abi.ERR_UNSUPPORTED and not h.value
+    assert b"4096" in _abi.lib().msosm_last_error()
+
+
+def test_tensor_layout_tables():
+    # host mirror of tc_pos (tc_layout.hpp) is a permutation of the 4096 bins,
+    # and the gather's thread mapping puts the bin pairs of one warp store in
+    # one 128-byte core matrix of the MN-major operand
+    def tc_pos(b):
+        k1, k2 = b & 63, b >> 6
+        u = (k1 >> 3) * 8 + (k2 >> 3)
+        l = (k2 & 7) * 4 + ((k1 & 7) >> 1)
+        return u * 64 + l * 2 + (k1 & 1)
+
+    def mn_off(r, k):
+        return (r >> 3) * 128 + (k >> 3) * 2048 + (k & 7) * 16 + (r & 7) * 2
+
+    pos = np.array([tc_pos(b) for b in range(4096)])
+    assert np.array_equal(np.sort(pos), np.arange(4096))
+    inv = np.argsort(pos)
+    for j in range(8):
+        for w in range(8):
+            offs = []
+            for lane in range(32):
+                b = inv[(j * 8 + w) * 64 + 2 * lane]
+                k1, k2 = b & 63, b >> 6
+                offs.append(mn_off(k1, k2))
+                assert inv[(j * 8 + w) * 64 + 2 * lane + 1] == b + 1
+            offs = np.array(offs)
+            assert np.array_equal(np.sort(offs), offs.min() + 4 * np.arange(32))
+            assert offs.min() % 128 == 0
+    # every operand element lies inside its 32 KB region
+    assert max(mn_off(r, k) for r in range(128) for k in range(128)) < 32768
+
+
 @pytest.mark.parametrize("k", range(len(META["msosm"])))
 def test_prepare_matches_reference(k):
     s = META["msosm"][k]

@@ -1,0 +1,150 @@
+"""Tensor-core (tcgen05) inverse transforms, MSOSM_FLAG_TENSOR_F16: each GEMM
+of the kernel on known data, then the dedispersed series and folded profiles
+against the FP64 oracle and against the FP32 CUDA-core path.
+
+Error budget (stated, not tuned): f16 operands carry a relative rounding of
+2^-11 at four places (gathered products, DFT constants, twiddled
+intermediates, second DFT constants), which gives a series error near 5e-4
+relative RMS; the tests bound it at 1.5e-3.  Folded profiles average many
+samples per bin and are bound at 1e-4."""
+import numpy as np
+import pytest
+
+import oracle as O
+from msosm_gpu_b200 import Dedisperser
+from msosm_gpu_b200.dedisp import tc_gemm_check
+
+pytestmark = pytest.mark.gpu
+
+BW, F0 = 16e6, 1242e6
+SERIES_TOL = 1.5e-3
+FOLD_TOL = 1e-4
+
+
+def rel_rms(a, b):
+    a, b = np.asarray(a), np.asarray(b)
+    return float(np.sqrt(np.mean(np.abs(a - b) ** 2) / np.mean(np.abs(b) ** 2)))
+
+
+def dft_operand(step):
+    """The real form of the 64-point inverse DFT the kernel multiplies by,
+    K x N with K = [Re | Im] of the input index, rounded to float16."""
+    if step == 1:
+        k = np.arange(64)[:, None]
+        m = np.arange(64)[None, :]
+    else:
+        k = np.arange(64)[:, None]
+        m = np.arange(32, 64)[None, :]
+    ang = 2 * np.pi * ((k * m) % 64) / 64
+    c, s = np.cos(ang), np.sin(ang)
+    B = np.block([[c, s], [-s, c]])
+    return B.astype(np.float16).astype(np.float64)
+
+
+@pytest.mark.parametrize("step", [1, 2])
+def test_gemm_layout_and_readback(step):
+    rng = np.random.default_rng(step)
+    a = rng.standard_normal((128, 128)).astype(np.float16)
+    d = tc_gemm_check(step, a)
+    ref = a.astype(np.float64) @ dft_operand(step)
+    err = np.max(np.abs(d - ref)) / np.max(np.abs(ref))
+    assert err < 1e-3, err
+
+
+def u16(n, seed, scale=1000.0):
+    rng = np.random.default_rng(seed)
+    return np.clip(np.rint(rng.standard_normal((n, 2)) * scale) + 32768, 1, 65535).astype(np.uint16)
+
+
+def run_pair(dms, count, calls, seed=0, series=True, x=None):
+    d = Dedisperser(BW, dms, F0, 4096, count, precision="fp16", series=series)
+    o = O.Dedisp(BW, dms, F0, 4096, count)
+    if x is None:
+        x = u16(d.block_samples * calls, seed)
+    ours, ref = [], []
+    for c in range(calls):
+        blk = x[c * d.block_samples:(c + 1) * d.block_samples]
+        d.filter_block(blk)
+        ours.append(d.get_output())
+        ref.append(o.filter(O.decode_uint16(blk)))
+    return np.concatenate(ours, 1), np.concatenate(ref, 1), d, x
+
+
+@pytest.mark.parametrize("count,calls", [(6, 3), (5, 4), (1, 5)])
+def test_series_matches_oracle(count, calls):
+    # DM 0 (no delay), short delays (warm ring after a few blocks) and long
+    # ones (blocks before the stream start read as zero); odd counts leave
+    # the last block of a call unpaired
+    dms = [0.0, 2.0, 5.0, 40.0, 100.0]
+    ours, ref, _, _ = run_pair(dms, count, calls, seed=count)
+    for i in range(len(dms)):
+        e = rel_rms(ours[i], ref[i])
+        assert e < SERIES_TOL, (dms[i], e)
+
+
+def test_series_matches_fp32_path():
+    dms = list(np.linspace(0, 100, 16))
+    count, calls = 8, 3
+    t = Dedisperser(BW, dms, F0, 4096, count, precision="fp16")
+    f = Dedisperser(BW, dms, F0, 4096, count)
+    x = u16(t.block_samples * calls, 11)
+    for c in range(calls):
+        blk = x[c * t.block_samples:(c + 1) * t.block_samples]
+        t.filter_block(blk)
+        f.filter_block(blk)
+        a, b = t.get_output(), f.get_output()
+        for i in range(len(dms)):
+            assert rel_rms(a[i], b[i]) < SERIES_TOL
+
+
+def test_zero_input_gives_zero():
+    d = Dedisperser(BW, [0.0, 50.0], F0, 4096, 4, precision="fp16")
+    x = np.full((d.block_samples, 2), 32768, np.uint16)
+    for _ in range(2):
+        d.filter_block(x)
+        assert not np.any(d.get_output())
+
+
+def test_full_scale_tone_stays_finite_and_accurate():
+    # a full-scale tone concentrates the spectrum in one bin: the per-block
+    # power-of-two scale must keep every f16 operand in range
+    d = Dedisperser(BW, [0.0, 30.0], F0, 4096, 4, precision="fp16")
+    o = O.Dedisp(BW, [0.0, 30.0], F0, 4096, 4)
+    n = d.block_samples * 3
+    t = np.arange(n)
+    z = 32000 * np.exp(2j * np.pi * 0.1234 * t)
+    x = np.stack([np.rint(z.real) + 32768, np.rint(z.imag) + 32768], 1).astype(np.uint16)
+    ours, ref = [], []
+    for c in range(3):
+        blk = x[c * d.block_samples:(c + 1) * d.block_samples]
+        d.filter_block(blk)
+        ours.append(d.get_output())
+        ref.append(o.filter(O.decode_uint16(blk)))
+    ours, ref = np.concatenate(ours, 1), np.concatenate(ref, 1)
+    assert np.all(np.isfinite(ours))
+    for i in range(2):
+        assert rel_rms(ours[i], ref[i]) < SERIES_TOL
+
+
+def test_fold_matches_oracle():
+    dms, count, calls, period, tb = [0.0, 20.0, 73.2], 8, 6, 0.0011, 256
+    d = Dedisperser(BW, dms, F0, 4096, count, series=False, precision="fp16")
+    nd = 4096
+    d.fold_init(period, BW, time_bin=tb, discard_Nd=nd)
+    o = O.Dedisp(BW, dms, F0, 4096, count)
+    x = u16(d.block_samples * calls, 21)
+    ser = []
+    for c in range(calls):
+        blk = x[c * d.block_samples:(c + 1) * d.block_samples]
+        d.filter_block(blk)
+        ser.append(o.filter(O.decode_uint16(blk)))
+    ser = np.concatenate(ser, 1)
+    prof = d.get_profiles()
+    assert d.folded_periods() > 0
+    for i in range(len(dms)):
+        f = O.Fold(period, BW, d.block_samples, tb)
+        f.discard_samples(nd)
+        for c in range(calls):
+            f.fold_data(np.abs(ser[i, c * d.block_samples:(c + 1) * d.block_samples]) ** 2)
+        e = rel_rms(prof[i], f.fold_data_bins())
+        assert e < FOLD_TOL, (dms[i], e)
