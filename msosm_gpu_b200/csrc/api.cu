@@ -239,7 +239,8 @@ cudaError_t plan_grid(msosm_dedisp *d)
         e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess)
         return e;
-    const size_t extra = d->fold ? fold_smem_bytes(d->nbins, d->win_cap, d->nbins <= kMaxSmemBins) : 0;
+    const int threads = d->tc ? tc::kThreads : (int)(d->N / 16);
+    const size_t extra = d->fold ? fold_smem_bytes(d->nbins, d->win_cap, d->nbins <= kMaxSmemBins, threads) : 0;
     int per_sm = d->tc ? tc_blocks_per_sm(d->series, d->fold, extra)
                        : dedisp_blocks_per_sm(d->log2n, d->pingpong, d->series, d->fold, extra);
     if (per_sm < 1)

@@ -9,15 +9,31 @@ namespace msosm {
 // Folding inside the dedispersion kernel.  The host fold planner cuts each
 // call's output samples into spans (one period each, sorted); a work item
 // keeps a window of them in shared memory and its two partial profiles
-// (complete periods, pending period) in shared memory too.  Every bin of a
-// span piece is summed by one warp (lanes strided over its samples, then a
-// fixed xor-butterfly) or, for bins of fewer than 16 samples, by one thread
-// in sample order; span pieces are separated by barriers.  The result does
-// not depend on scheduling.
+// (complete periods, pending period) in shared memory too.  A block of 8
+// samples per thread that lies inside one span, with at least 8 samples per
+// output bin, takes the fast path: each thread sums its 8 consecutive
+// samples into at most two bin partials, and a group of lanes per bin adds
+// that bin's partials in thread order.  Other blocks go span piece by span
+// piece: every bin is summed by a group of lanes strided over its samples.
+// Either way the summation order is fixed, so the result does not depend on
+// scheduling.
 struct FoldSmem {
     float *prof_main, *prof_pend;  // [nbins] each (or the global rows)
     int *wa, *wb, *wp, *wd;        // span window (chunk-local sample indices < 2^31)
+    float *pa;                     // [2][threads] per-thread bin partials of the fast path
 };
+
+// Shared-memory layout of the fold state at `base` (sized by fold_smem_bytes).
+__device__ __forceinline__ void fold_smem_layout(FoldSmem &w, void *base, const FoldArgs &f)
+{
+    w.wa = reinterpret_cast<int *>(base);
+    w.wb = w.wa + f.span_cap;
+    w.wp = w.wb + f.span_cap;
+    w.wd = w.wp + f.span_cap;
+    w.pa = reinterpret_cast<float *>(w.wd + f.span_cap);
+    w.prof_main = w.pa + 2 * blockDim.x;
+    w.prof_pend = w.prof_main + f.nbins;
+}
 
 __device__ __forceinline__ int span_lower_bound(const long long *b, int n, long long t)
 {
@@ -65,7 +81,11 @@ __device__ __forceinline__ int div_bpt(int x, int bpt, float inv_bpt)
 // ibuf holds intensities at index t + t/32 (one pad slot per 32 samples), so
 // that threads reading bins of any length hit different banks
 __device__ __forceinline__ int ipad(int t) { return t + (t >> 5); }
+// the intensity buffer index of sample t: padded (PAD) or plain
+template <bool PAD>
+__device__ __forceinline__ int iidx(int t) { return PAD ? ipad(t) : t; }
 
+template <bool PAD>
 __device__ __forceinline__ void fold_piece(const FoldArgs &f, float *prof, const float *ibuf, int off,
                                            int ph_lo, int ph_hi)
 {
@@ -93,11 +113,11 @@ __device__ __forceinline__ void fold_piece(const FoldArgs &f, float *prof, const
             const int s_hi = min(ph_hi, s0 + f.bpt);
             int p = s_lo + l;
             for (; p + G < s_hi; p += 2 * G) {
-                a0 += ibuf[ipad(off + p)];
-                a1 += ibuf[ipad(off + p + G)];
+                a0 += ibuf[iidx<PAD>(off + p)];
+                a1 += ibuf[iidx<PAD>(off + p + G)];
             }
             if (p < s_hi)
-                a0 += ibuf[ipad(off + p)];
+                a0 += ibuf[iidx<PAD>(off + p)];
         }
         float sum = a0 + a1;
         for (int o = G >> 1; o > 0; o >>= 1)
@@ -107,8 +127,95 @@ __device__ __forceinline__ void fold_piece(const FoldArgs &f, float *prof, const
     }
 }
 
+// Fast path of fold_block: the block's M = 8 * blockDim.x samples all lie in
+// one span (phases ph_lo .. ph_lo + M - 1), bpt >= 8, so a thread's 8
+// samples touch at most two bins.  Samples whose bin is past the last output
+// bin are not folded (n_valid of them are).  Each thread sums its samples of
+// its first bin (and of the next one); every bin is then completed by the
+// thread holding its first sample (thread 0 for the bin running into the
+// block), adding the following threads' first-bin sums in thread order.
+template <bool PAD>
+__device__ __forceinline__ void fold_block_fast(const FoldArgs &f, FoldSmem &w, float *prof, const float *ibuf,
+                                                int ph_lo, int n_valid)
+{
+    const int tid = threadIdx.x, T = blockDim.x;
+    const int bpt = f.bpt;
+    const int j0 = 8 * tid;
+    const int ph = ph_lo + j0;
+    const int b0 = div_bpt(ph, bpt, f.inv_bpt);
+    const int r0 = ph - b0 * bpt;  // place of the first sample in its bin
+    const int n0 = bpt - r0;       // samples left in bin b0 (>= 1)
+    const int nv = min(8, n_valid - j0);
+    float x[8];
+    if constexpr (PAD) {
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+            x[u] = ibuf[ipad(j0 + u)];
+    } else {
+        const float4 lo = reinterpret_cast<const float4 *>(ibuf)[2 * tid];
+        const float4 hi = reinterpret_cast<const float4 *>(ibuf)[2 * tid + 1];
+        x[0] = lo.x; x[1] = lo.y; x[2] = lo.z; x[3] = lo.w;
+        x[4] = hi.x; x[5] = hi.y; x[6] = hi.z; x[7] = hi.w;
+    }
+    float s0 = 0.f, s1 = 0.f;
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+        const float v = u < nv ? x[u] : 0.f;
+        if (u < n0)
+            s0 += v;
+        else
+            s1 += v;
+    }
+    w.pa[tid] = s0;
+    w.pa[T + tid] = s1;
+    __syncthreads();
+    if (bpt <= 256) {
+        // bin B starting at this thread, first sums acc: add the first-bin sums
+        // of the threads up to the bin's end
+        auto finish = [&](int B, float acc) {
+            const int e = min((B + 1) * bpt - ph_lo, n_valid);
+            for (int t = tid + 1; 8 * t < e; ++t)
+                acc += w.pa[t];
+            prof[B] += acc;
+        };
+        if (nv > 0) {
+            if (tid == 0 && r0 != 0)
+                finish(b0, s0);
+            if (r0 == 0)
+                finish(b0, s0);
+            else if (n0 < nv)
+                finish(b0 + 1, s1);
+        }
+        return;
+    }
+    // long bins: G lanes per bin over the threads ta..tb that hold its samples
+    // (first bin B when the thread's first phase is >= B*bpt, else its second)
+    int g2 = 0;
+    while (g2 < 5 && (4 << g2) < (bpt >> 3) + 2)
+        ++g2;
+    const int G = 1 << g2, g = tid >> g2, l = tid & (G - 1), ngroups = T >> g2;
+    const int b_first = div_bpt(ph_lo, bpt, f.inv_bpt);
+    const int b_last = div_bpt(ph_lo + n_valid - 1, bpt, f.inv_bpt);
+    for (int first = b_first; first <= b_last; first += ngroups) {
+        const int B = first + g;
+        float sum = 0.f;
+        if (B <= b_last) {
+            const int lo = B * bpt - ph_lo;
+            const int ta = lo > 0 ? (lo >> 3) : 0;
+            const int tb = min((B + 1) * bpt - 1 - ph_lo, n_valid - 1) >> 3;
+            for (int t = ta + l; t <= tb; t += G)
+                sum += (8 * t >= lo) ? w.pa[t] : w.pa[T + t];
+        }
+        for (int o = G >> 1; o > 0; o >>= 1)
+            sum += __shfl_xor_sync(0xffffffffu, sum, o);
+        if (B <= b_last && l == 0)
+            prof[B] += sum;
+    }
+}
+
 // Fold the M intensities of one block (ibuf: chunk-local samples t0..t0+M-1).
 // sp/base/cnt: the work item's running span cursor and window (uniform).
+template <bool PAD>
 __device__ __forceinline__ void fold_block(const FoldArgs &f, FoldSmem &w, const float *ibuf, int t0, int M,
                                            int &sp, int &base, int &cnt)
 {
@@ -120,6 +227,20 @@ __device__ __forceinline__ void fold_block(const FoldArgs &f, FoldSmem &w, const
             ++sp;
         else
             break;
+    }
+    if (sp < f.nspans && f.bpt >= 8 && M == 8 * (int)blockDim.x) {
+        const int i = sp - base;
+        const int sa = w.wa[i];
+        if (sa <= t0 && w.wb[i] >= t0 + M) {
+            const int dest = w.wd[i];
+            if (dest != 0) {
+                const int ph_lo = w.wp[i] + (t0 - sa);
+                const int n_valid = min(M, f.nbins * f.bpt - ph_lo);
+                if (n_valid > 0)
+                    fold_block_fast<PAD>(f, w, dest == 1 ? w.prof_main : w.prof_pend, ibuf, ph_lo, n_valid);
+            }
+            return;
+        }
     }
     const int t1 = t0 + M;
     for (int s = sp; s < f.nspans; ++s) {
@@ -135,7 +256,7 @@ __device__ __forceinline__ void fold_block(const FoldArgs &f, FoldSmem &w, const
             const int a = max(sa, t0), b = min(sb, t1);
             if (a < b) {
                 const int ph_lo = w.wp[i] + (a - sa);
-                fold_piece(f, dest == 1 ? w.prof_main : w.prof_pend, ibuf, a - t0 - ph_lo, ph_lo, ph_lo + (b - a));
+                fold_piece<PAD>(f, dest == 1 ? w.prof_main : w.prof_pend, ibuf, a - t0 - ph_lo, ph_lo, ph_lo + (b - a));
             }
             // a later span of this block may fold into the same bins
             if (sb < t1)

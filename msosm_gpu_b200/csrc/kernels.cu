@@ -124,13 +124,8 @@ __global__ void __launch_bounds__(FftShape<LOG2N>::T) dedisp_kernel(DedispArgs a
     float *ibuf = reinterpret_cast<float *>(smem + (PP ? 2 : 1) * F::SMEM);
     FoldSmem fw;
     if constexpr (FOLD) {
-        // after ibuf: [span window a, b, phase0, dest] [prof_main, prof_pend]
-        fw.wa = reinterpret_cast<int *>(ibuf + ibuf_floats(M));
-        fw.wb = fw.wa + a.fold.span_cap;
-        fw.wp = fw.wb + a.fold.span_cap;
-        fw.wd = fw.wp + a.fold.span_cap;
-        fw.prof_main = reinterpret_cast<float *>(fw.wd + a.fold.span_cap);
-        fw.prof_pend = fw.prof_main + a.fold.nbins;
+        // after ibuf: [span window a, b, phase0, dest] [partials] [prof_main, prof_pend]
+        fold_smem_layout(fw, ibuf + ibuf_floats(M), a.fold);
     }
     const int tid = threadIdx.x;
     const int items = a.D * a.R;
@@ -200,7 +195,7 @@ __global__ void __launch_bounds__(FftShape<LOG2N>::T) dedisp_kernel(DedispArgs a
             }
             if constexpr (FOLD) {
                 __syncthreads();
-                fold_block(a.fold, fw, ibuf, k * M, M, sp, sbase, scnt);
+                fold_block<true>(a.fold, fw, ibuf, k * M, M, sp, sbase, scnt);
             }
         }
         if constexpr (FOLD) {
@@ -251,12 +246,7 @@ __global__ void __launch_bounds__(256) fold_series_kernel(const float *__restric
     extern __shared__ float2 smem[];
     float *ibuf = reinterpret_cast<float *>(smem);
     FoldSmem fw;
-    fw.wa = reinterpret_cast<int *>(ibuf + ibuf_floats(kFoldBlock));
-    fw.wb = fw.wa + f.span_cap;
-    fw.wp = fw.wb + f.span_cap;
-    fw.wd = fw.wp + f.span_cap;
-    fw.prof_main = reinterpret_cast<float *>(fw.wd + f.span_cap);
-    fw.prof_pend = fw.prof_main + f.nbins;
+    fold_smem_layout(fw, ibuf + ibuf_floats(kFoldBlock), f);
     const long long nblk = (n + kFoldBlock - 1) / kFoldBlock;
     for (int w = blockIdx.x; w < R; w += gridDim.x) {
         const long long kb = nblk * w / R, ke = nblk * (w + 1) / R;
@@ -274,7 +264,7 @@ __global__ void __launch_bounds__(256) fold_series_kernel(const float *__restric
             for (int t = threadIdx.x; t < kFoldBlock; t += blockDim.x)
                 ibuf[ipad(t)] = (long long)t0 + t < n ? I[t0 + t] : 0.f;
             __syncthreads();
-            fold_block(f, fw, ibuf, t0, kFoldBlock, sp, sbase, scnt);
+            fold_block<true>(f, fw, ibuf, t0, kFoldBlock, sp, sbase, scnt);
             __syncthreads();
         }
         if (f.smem_prof) {
@@ -450,9 +440,9 @@ static cudaError_t forward_t(InputKind kind, const FwdArgs &a, cudaStream_t st)
     return cudaGetLastError();
 }
 
-size_t fold_smem_bytes(int nbins, int span_cap, bool smem_prof)
+size_t fold_smem_bytes(int nbins, int span_cap, bool smem_prof, int threads)
 {
-    return (size_t)span_cap * 4 * sizeof(int) +
+    return (size_t)span_cap * 4 * sizeof(int) + 2 * (size_t)threads * sizeof(float) +
            (smem_prof ? 2 * (size_t)nbins * sizeof(float) : 0);
 }
 
@@ -482,7 +472,8 @@ static cudaError_t dedisp_t(bool pp, bool series, bool fold, const DedispArgs &a
 {
     pp = pp && use_pingpong<LOG2N>();
     const size_t sm = dedisp_smem_bytes<LOG2N>(pp) +
-                      (fold ? fold_smem_bytes(a.fold.nbins, a.fold.span_cap, a.fold.smem_prof != 0) : 0);
+                      (fold ? fold_smem_bytes(a.fold.nbins, a.fold.span_cap, a.fold.smem_prof != 0,
+                                              FftShape<LOG2N>::T) : 0);
     return dedisp_select<LOG2N>(pp, series, fold, [&](auto k) -> cudaError_t {
         cudaError_t e = set_smem(k, sm);
         if (e != cudaSuccess)
@@ -600,7 +591,8 @@ int fold_series_block() { return kFoldBlock; }
 cudaError_t launch_fold_series(const float *I, long long n, int R, const FoldArgs &f, int grid, int trials,
                                cudaStream_t st)
 {
-    const size_t sm = ibuf_floats(kFoldBlock) * sizeof(float) + fold_smem_bytes(f.nbins, f.span_cap, f.smem_prof != 0);
+    const size_t sm =
+        ibuf_floats(kFoldBlock) * sizeof(float) + fold_smem_bytes(f.nbins, f.span_cap, f.smem_prof != 0, 256);
     cudaError_t e = set_smem(fold_series_kernel, sm);
     if (e != cudaSuccess)
         return e;

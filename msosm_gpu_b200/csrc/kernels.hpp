@@ -54,8 +54,8 @@ inline int fold_g_shift(int bpt, int threads)
 // intensity staging of one block: M samples, one pad slot per 32
 __host__ __device__ constexpr int ibuf_floats(int m) { return (m + (m >> 5) + 1) & ~1; }
 
-// Extra dynamic shared memory of the folding dedispersion kernel.
-size_t fold_smem_bytes(int nbins, int span_cap, bool smem_prof);
+// Extra dynamic shared memory of the folding dedispersion kernel (threads: its block size).
+size_t fold_smem_bytes(int nbins, int span_cap, bool smem_prof, int threads);
 constexpr int kMaxSmemBins = 4096;
 
 struct DedispArgs {

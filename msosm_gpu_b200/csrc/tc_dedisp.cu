@@ -12,11 +12,13 @@
 // tc_layout.hpp): GEMM 1 (M 128 = 2 blocks x 64 k1, N 128, K 128), a twiddle
 // pass on the CUDA cores, GEMM 2 (M 128 = 2 blocks x 64 m2, N 64, K 128).
 //
-// Precision: the gathered products of a block pair are scaled by a power of
-// two chosen so that no component can reach 2^8 -- from the largest
-// component of every ring row the pair reads (recorded by the forward
-// kernel) times the trial's largest filter component -- so every GEMM 1 sum
-// stays below 2^15 and every twiddled value below 2^15.5, inside f16.  The
+// Precision: the gathered products of a work item (one trial, a range of
+// blocks) are scaled by a power of two chosen so that no component can reach
+// 2^8 -- from the largest component of every ring row the item reads
+// (recorded by the forward kernel) times the trial's largest filter
+// component -- so every GEMM 1 sum stays below 2^15 and every twiddled value
+// below 2^15.5, inside f16; f16's 2^-24..2^16 range leaves quiet stretches
+// far from underflow unless a burst in the range is ~10^6 times stronger.  The
 // twiddle multiply runs in f16 arithmetic on f16-rounded twiddles.  The
 // scale is undone exactly on the f32 results.
 //
@@ -38,6 +40,8 @@ namespace {
 using namespace tc;
 
 constexpr unsigned long long kWaitLimitNs = 1000000000ull;
+// try_wait sleeps up to this long (or until the phase completes) per attempt
+constexpr uint32_t kSuspendHintNs = 100000u;
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -56,10 +60,10 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity)
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(ok)
-        : "r"(bar), "r"(parity)
+        : "r"(bar), "r"(parity), "r"(kSuspendHintNs)
         : "memory");
     return ok != 0;
 }
@@ -168,47 +172,44 @@ __device__ __forceinline__ float warp_max(float v)
     return v;
 }
 
-// The constant operands: the 64-point inverse DFT in real form.
-//   GEMM 1, B1[n][kk]: n < 64 -> Re A[m2 = n], n >= 64 -> Im A[m2 = n - 64];
-//     kk < 64 -> Re Z[k2 = kk], kk >= 64 -> Im Z[k2 = kk - 64]
-//   GEMM 2, B2[n][kk]: n < 32 -> Re y[m1 = 32 + n], n >= 32 -> Im y[m1 = n];
-//     kk < 64 -> Re A'[k1 = kk], kk >= 64 -> Im A'[k1 = kk - 64]
+// The constant operands: [C | S] of the 64-point inverse DFT, K-major.
+//   GEMM 1, B1[n][k2], k2 < 64: n < 64 -> cos(2 pi k2 n / 64),
+//     n >= 64 -> sin(2 pi k2 (n - 64) / 64)            (output frequency m2)
+//   GEMM 2, B2[n][k1], k1 < 64: n < 32 -> cos(2 pi k1 (32 + n) / 64),
+//     n >= 32 -> sin(2 pi k1 n / 64)                   (output m1 = 32..63)
 __device__ void fill_constants(unsigned char *sm, int tid)
 {
-    for (int e = tid; e < 128 * 128; e += kThreads) {
-        const int n = e >> 7, kk = e & 127;
-        const int k2 = kk & 63, m2 = n & 63;
+    for (int e = tid; e < 128 * 64; e += kThreads) {
+        const int n = e >> 6, k = e & 63;
         float s, c;
-        sincospif((float)((k2 * m2) & 63) * (1.0f / 32.0f), &s, &c);
-        const float v = kk < 64 ? (n < 64 ? c : s) : (n < 64 ? -s : c);
-        *reinterpret_cast<__half *>(sm + kSmemBA + k_off(n, kk)) = __float2half_rn(v);
+        sincospif((float)((k * (n & 63)) & 63) * (1.0f / 32.0f), &s, &c);
+        *reinterpret_cast<__half *>(sm + kSmemB1 + k_off(n, k)) = __float2half_rn(n < 64 ? c : s);
     }
-    for (int e = tid; e < 64 * 128; e += kThreads) {
-        const int n = e >> 7, kk = e & 127;
-        const int k1 = kk & 63, m1 = 32 + (n & 31);
+    for (int e = tid; e < 64 * 64; e += kThreads) {
+        const int n = e >> 6, k = e & 63;
         float s, c;
-        sincospif((float)((k1 * m1) & 63) * (1.0f / 32.0f), &s, &c);
-        const float v = kk < 64 ? (n < 32 ? c : s) : (n < 32 ? -s : c);
-        *reinterpret_cast<__half *>(sm + kSmemBC + k_off(n, kk)) = __float2half_rn(v);
+        sincospif((float)((k * (32 + (n & 31))) & 63) * (1.0f / 32.0f), &s, &c);
+        *reinterpret_cast<__half *>(sm + kSmemB2 + k_off(n, k)) = __float2half_rn(n < 32 ? c : s);
     }
 }
 
-// mbarrier + tensor memory; every thread returns the TMEM base address
+// mbarriers (GEMM 1, GEMM 2) + tensor memory; every thread returns the TMEM base
 __device__ uint32_t tc_setup(unsigned char *sm, uint32_t s0, int tid, int warp)
 {
     if (tid == 0) {
         mbar_init(s0 + kSmemCtl, 1);
+        mbar_init(s0 + kSmemCtl + 8, 1);
         fence_mbar_init();
     }
     if (warp == 0) {
-        tmem_alloc(s0 + kSmemCtl + 8, kTmemCols);
+        tmem_alloc(s0 + kSmemCtl + 16, kTmemCols);
         tmem_relinquish();
     }
     fence_proxy_async();  // shared-memory operands written so far -> tensor core
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    return *reinterpret_cast<volatile uint32_t *>(sm + kSmemCtl + 8);
+    return *reinterpret_cast<volatile uint32_t *>(sm + kSmemCtl + 16);
 }
 
 __device__ __forceinline__ void tc_teardown(uint32_t tmem, int warp)
@@ -221,17 +222,43 @@ __device__ __forceinline__ void tc_teardown(uint32_t tmem, int warp)
     }
 }
 
-// eight K = 16 steps of one GEMM, then the commit to the mbarrier
-__device__ __forceinline__ void issue_gemm(uint32_t tmem_d, uint32_t a_addr, uint32_t b_addr, uint32_t idesc,
-                                           uint32_t bar)
+// One complex GEMM: D (n2 = 2 * half columns: [Re | Im]) = data (128 x [Re |
+// Im] K = 128, MN-major at a) x the DFT whose [C | S] (K = 64, n2 columns)
+// is at b; then the commit to the mbarrier.  Three passes of four K = 16
+// steps: Re x [C | S], then -Im x S into the Re half, Im x C into the Im half.
+__device__ __forceinline__ void issue_cgemm(uint32_t tmem_d, uint32_t a, uint32_t b, int half, uint32_t bar)
 {
+    const uint32_t id_full = idesc_f16(128, 2 * half, true);
+    const uint32_t id_neg = idesc_f16(128, half, true, true);
+    const uint32_t id_half = idesc_f16(128, half, true);
 #pragma unroll
-    for (int s = 0; s < 8; ++s) {
-        const uint64_t da = smem_desc(a_addr + s * kDescStepA, 2048, 128);
-        const uint64_t db = smem_desc(b_addr + s * kDescStepB, 128, 2048);
-        mma_f16(tmem_d, da, db, idesc, s > 0 ? 1u : 0u);
-    }
+    for (int s = 0; s < 4; ++s)
+        mma_f16(tmem_d, smem_desc(a + s * kDescStepA, 2048, 128), smem_desc(b + s * kDescStepB, 128, 1024),
+                id_full, s > 0 ? 1u : 0u);
+#pragma unroll
+    for (int s = 0; s < 4; ++s)
+        mma_f16(tmem_d, smem_desc(a + (4 + s) * kDescStepA, 2048, 128),
+                smem_desc(b + b_col(half) + s * kDescStepB, 128, 1024), id_neg, 1u);
+#pragma unroll
+    for (int s = 0; s < 4; ++s)
+        mma_f16(tmem_d + half, smem_desc(a + (4 + s) * kDescStepA, 2048, 128),
+                smem_desc(b + s * kDescStepB, 128, 1024), id_half, 1u);
     mma_commit(bar);
+}
+
+// Thread 0 waits for a commit (bounded); every thread learns the outcome.
+// Returns false (uniformly) on a timeout; parity then still names the
+// phase waited for.
+__device__ __forceinline__ bool wait_gemm(int tid, uint32_t bar, uint32_t &parity)
+{
+    bool ok = true;
+    if (tid == 0)
+        ok = mbar_wait(bar, parity, kWaitLimitNs);
+    const bool failed = __syncthreads_or(!ok);
+    if (!failed)
+        parity ^= 1;
+    tc_fence_after();
+    return !failed;
 }
 
 template <bool SERIES, bool FOLD>
@@ -240,19 +267,10 @@ __global__ void __launch_bounds__(kThreads, 2) tc_dedisp_kernel(DedispArgs a)
     extern __shared__ __align__(1024) unsigned char sm[];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t s0 = smem_addr(sm);
-    const uint32_t bar = s0 + kSmemCtl;
-    unsigned char *op = sm + kSmemOp;
-    float *ibuf0 = reinterpret_cast<float *>(sm + kSmemOp);
-    float *ibuf1 = ibuf0 + ibuf_floats(kM);
+    const uint32_t barA = s0 + kSmemCtl, barB = s0 + kSmemCtl + 8;
     FoldSmem fw;
-    if constexpr (FOLD) {
-        fw.wa = reinterpret_cast<int *>(sm + kSmemFold);
-        fw.wb = fw.wa + a.fold.span_cap;
-        fw.wp = fw.wb + a.fold.span_cap;
-        fw.wd = fw.wp + a.fold.span_cap;
-        fw.prof_main = reinterpret_cast<float *>(fw.wd + a.fold.span_cap);
-        fw.prof_pend = fw.prof_main + a.fold.nbins;
-    }
+    if constexpr (FOLD)
+        fold_smem_layout(fw, sm + kSmemFold, a.fold);
     fill_constants(sm, tid);
     const uint32_t tmem = tc_setup(sm, s0, tid, warp);
     // epilogue view: warp w reads TMEM lanes 32 (w % 4) .. + 31 (its GEMM
@@ -280,24 +298,49 @@ __global__ void __launch_bounds__(kThreads, 2) tc_dedisp_kernel(DedispArgs a)
     const int items = a.D * a.R;
     const int npairs = (a.count + 1) >> 1;
     const int smask = a.S - 1;
-    uint32_t phase = 0;
+    uint32_t phA = 0, phB = 0;
+    bool pendA = false, pendB = false;  // a commit not yet waited for
     bool failed = false;
-    for (int w = blockIdx.x; w < items; w += gridDim.x) {
+    for (int w = blockIdx.x; w < items && !failed; w += gridDim.x) {
         const int dm = w % a.D;
         const int rr = w / a.D;
         const int kb = 2 * (int)((long long)npairs * rr / a.R);
         const int ke = min(a.count, 2 * (int)((long long)npairs * (rr + 1) / a.R));
-        const float4 *__restrict__ H4 = reinterpret_cast<const float4 *>(a.H + (size_t)dm * kN);
-        // this thread's bin-pair delays are fixed for the trial
+        const int np = (ke - kb + 1) >> 1;
+        // this thread's bin pairs: filter values and delays, fixed for the trial
+        float4 hreg[8];
         uint32_t dd[8];
         {
+            const float4 *__restrict__ H4 = reinterpret_cast<const float4 *>(a.H + (size_t)dm * kN);
             const uint32_t *__restrict__ dl2 = reinterpret_cast<const uint32_t *>(a.delays + (size_t)dm * kN);
 #pragma unroll
-            for (int j = 0; j < 8; ++j)
+            for (int j = 0; j < 8; ++j) {
                 dd[j] = __ldg(dl2 + (j * 8 + warp) * 32 + lane);
+                hreg[j] = __ldg(H4 + (j * 8 + warp) * 32 + lane);
+            }
         }
-        const float hmx = __ldg(a.h_max + dm);
-        const int nrow = __ldg(a.delay_max + dm) + 2;
+        // power-of-two scale of the work item: |Z| <= 2 max|X| max|H| over
+        // every ring row its blocks read (rows k0 + kb - largest delay .. k0 + ke - 1)
+        float sc, isc;
+        {
+            float wm = 0.f;
+            const long long r_hi = a.k0 + ke - 1;
+            for (long long r = a.k0 + kb - __ldg(a.delay_max + dm) + tid; r <= r_hi; r += kThreads)
+                if (r >= 0)
+                    wm = fmaxf(wm, a.row_max[r & smask]);
+            wm = warp_max(wm);
+            float *wmax = reinterpret_cast<float *>(sm + kSmemCtl + 32);
+            if (lane == 0)
+                wmax[warp] = wm;
+            __syncthreads();
+#pragma unroll
+            for (int i = 0; i < kThreads / 32; ++i)
+                wm = fmaxf(wm, wmax[i]);
+            pow2_scale(2.0f * wm * __ldg(a.h_max + dm), sc, isc);
+#pragma unroll
+            for (int j = 0; j < 8; ++j)
+                hreg[j] = make_float4(hreg[j].x * sc, hreg[j].y * sc, hreg[j].z * sc, hreg[j].w * sc);
+        }
         int sp = 0, sbase = 0, scnt = 0;
         if constexpr (FOLD) {
             if (a.fold.smem_prof) {
@@ -310,77 +353,82 @@ __global__ void __launch_bounds__(kThreads, 2) tc_dedisp_kernel(DedispArgs a)
             sp = span_lower_bound(a.fold.span_b, a.fold.nspans, (long long)kb * kM);
             span_refill(a.fold, fw, sp, sbase, scnt);
         }
-        for (int k = kb; k < ke; k += 2) {
+
+        // Gather pair i of the item (blocks k, k + 1) into operand buffer
+        // `op`: Z = X[kg + b - delay][bin] * H[bin] * sc, element (row 64 b
+        // + k1, k = k2) of the MN-major operand, Im parts 8 core-matrix
+        // columns on.
+        auto gather = [&](int i, unsigned char *op) {
+            const int k = kb + 2 * i;
             const bool two = k + 1 < ke;
             const long long kg = a.k0 + k;
-            const bool warm = kg >= a.max_delay;
             const int slot0 = (int)(kg & smask);
-            // ---- power-of-two scale of the pair: |Z| <= 2 max|X| max|H| over
-            // the ring rows kg + 1 - j (j <= largest delay + 1) it reads
-            float wm = 0.f;
-            for (int j = lane; j < nrow; j += 32) {
-                const long long r = kg + 1 - j;
-                if (r >= 0 && (j > 0 || two))
-                    wm = fmaxf(wm, a.row_max[r & smask]);
-            }
-            wm = warp_max(wm);
-            float sc, isc;
-            pow2_scale(2.0f * wm * hmx, sc, isc);
-            // ---- gather Z = X[kg + b - delay][bin] * H[bin] * sc of both
-            // blocks into the f16 operand of GEMM 1
+            if (kg >= a.max_delay && two) {
+                // every delayed block exists: no zero fill
 #pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                const int q = (j * 8 + warp) * 32 + lane;  // float4 (bin pair) index in a row
-                float4 hv = __ldg(H4 + q);
-                hv.x *= sc;
-                hv.y *= sc;
-                hv.z *= sc;
-                hv.w *= sc;
-                const int d0 = (int)(dd[j] & 0xFFFFu), d1 = (int)(dd[j] >> 16);
+                for (int j = 0; j < 8; ++j) {
+                    const int q = (j * 8 + warp) * 32 + lane;  // float4 (bin pair) index in a row
+                    const float4 hv = hreg[j];
+                    const int d0 = (int)(dd[j] & 0xFFFFu), d1 = (int)(dd[j] >> 16);
+                    float4 x[2];
+                    if (d0 == d1) {
+                        const int r = (slot0 - d0) & smask;
+                        x[0] = ring4[(size_t)r * (kN / 2) + q];
+                        x[1] = ring4[(size_t)((r + 1) & smask) * (kN / 2) + q];
+                    } else {
+                        const int r0 = (slot0 - d0) & smask, r1 = (slot0 - d1) & smask;
 #pragma unroll
-                for (int b = 0; b < 2; ++b) {
-                    float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
-                    if (b == 0 || two) {
-                        const long long kk = kg + b;
-                        if (d0 == d1) {
-                            if (warm || kk >= d0)  // blocks before the stream start are zero
-                                x = ring4[(size_t)((slot0 + b - d0) & smask) * (kN / 2) + q];
-                        } else {
-                            if (warm || kk >= d0) {
+                        for (int b = 0; b < 2; ++b) {
+                            const float2 t0 = ring2[(size_t)((r0 + b) & smask) * kN + 2 * q];
+                            const float2 t1 = ring2[(size_t)((r1 + b) & smask) * kN + 2 * q + 1];
+                            x[b] = make_float4(t0.x, t0.y, t1.x, t1.y);
+                        }
+                    }
+#pragma unroll
+                    for (int b = 0; b < 2; ++b) {
+                        const float zr0 = x[b].x * hv.x - x[b].y * hv.y, zi0 = x[b].x * hv.y + x[b].y * hv.x;
+                        const float zr1 = x[b].z * hv.z - x[b].w * hv.w, zi1 = x[b].z * hv.w + x[b].w * hv.z;
+                        const int off = (b * 8 + j) * 128 + warp * 2048 + (lane >> 2) * 16 + (lane & 3) * 4;
+                        *reinterpret_cast<uint32_t *>(op + off) = pack_half2(zr0, zr1);
+                        *reinterpret_cast<uint32_t *>(op + off + 8 * 2048) = pack_half2(zi0, zi1);
+                    }
+                }
+            } else {
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const int q = (j * 8 + warp) * 32 + lane;
+                    const float4 hv = hreg[j];
+                    const int d0 = (int)(dd[j] & 0xFFFFu), d1 = (int)(dd[j] >> 16);
+#pragma unroll
+                    for (int b = 0; b < 2; ++b) {
+                        float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
+                        if (b == 0 || two) {
+                            const long long kk = kg + b;
+                            // blocks before the stream start are zero
+                            if (kk >= d0) {
                                 const float2 t = ring2[(size_t)((slot0 + b - d0) & smask) * kN + 2 * q];
                                 x.x = t.x;
                                 x.y = t.y;
                             }
-                            if (warm || kk >= d1) {
+                            if (kk >= d1) {
                                 const float2 t = ring2[(size_t)((slot0 + b - d1) & smask) * kN + 2 * q + 1];
                                 x.z = t.x;
                                 x.w = t.y;
                             }
                         }
+                        const float zr0 = x.x * hv.x - x.y * hv.y, zi0 = x.x * hv.y + x.y * hv.x;
+                        const float zr1 = x.z * hv.z - x.w * hv.w, zi1 = x.z * hv.w + x.w * hv.z;
+                        const int off = (b * 8 + j) * 128 + warp * 2048 + (lane >> 2) * 16 + (lane & 3) * 4;
+                        *reinterpret_cast<uint32_t *>(op + off) = pack_half2(zr0, zr1);
+                        *reinterpret_cast<uint32_t *>(op + off + 8 * 2048) = pack_half2(zi0, zi1);
                     }
-                    const float zr0 = x.x * hv.x - x.y * hv.y, zi0 = x.x * hv.y + x.y * hv.x;
-                    const float zr1 = x.z * hv.z - x.w * hv.w, zi1 = x.z * hv.w + x.w * hv.z;
-                    // element (row 64 b + k1, k = k2) of the MN-major operand
-                    const int off = (b * 8 + j) * 128 + warp * 2048 + (lane >> 2) * 16 + (lane & 3) * 4;
-                    *reinterpret_cast<uint32_t *>(op + off) = pack_half2(zr0, zr1);
-                    *reinterpret_cast<uint32_t *>(op + off + 8 * 2048) = pack_half2(zi0, zi1);
                 }
             }
-            fence_proxy_async();
-            __syncthreads();
-            bool ok = true;
-            if (tid == 0) {
-                tc_fence_after();
-                issue_gemm(tmem, s0 + kSmemOp, s0 + kSmemBA, kIdesc1, bar);
-                ok = mbar_wait(bar, phase, kWaitLimitNs);
-            }
-            phase ^= 1;
-            if (__syncthreads_or(!ok)) {
-                failed = true;
-                break;
-            }
-            tc_fence_after();
-            // ---- twiddle D1 (f16 arithmetic) into the f16 operand of GEMM 2
+        };
+
+        // D1 -> twiddle (f16 arithmetic) -> f16 operand of GEMM 2 in `op`
+        // (rows 64 rb + m2, m2 = 32 h + 16 p + 8 g + 0..7; k = k1 (Re), 64 + k1 (Im))
+        auto twiddle = [&](unsigned char *op) {
 #pragma unroll
             for (int p = 0; p < 2; ++p) {
                 float re[16], im[16];
@@ -398,62 +446,120 @@ __global__ void __launch_bounds__(kThreads, 2) tc_dedisp_kernel(DedispArgs a)
                 }
 #pragma unroll
                 for (int g = 0; g < 2; ++g) {
-                    // rows 64 rb + m2 (m2 = 32 h + 16 p + 8 g + 0..7), k = k1 (Re), 64 + k1 (Im)
                     const int off = (rb * 8 + 4 * h + 2 * p + g) * 128 + (ri >> 3) * 2048 + (ri & 7) * 16;
                     st_shared_v4(op + off, pr[4 * g], pr[4 * g + 1], pr[4 * g + 2], pr[4 * g + 3]);
                     st_shared_v4(op + off + 8 * 2048, pim[4 * g], pim[4 * g + 1], pim[4 * g + 2], pim[4 * g + 3]);
                 }
             }
+        };
+
+        // D2 -> outputs m = M + 64 c + m2 (c = 16 h + u) of pair i: series,
+        // detection into the intensity buffers (kM floats per block, in `op`)
+        auto outputs = [&](int i, unsigned char *op) {
+            const int k = kb + 2 * i;
+            float yr[16], yi[16];
+            tmem_ld_2x16(tD2 + 16 * h, tD2 + 32 + 16 * h, yr, yi);
+            if constexpr (SERIES) {
+                if (rb == 0 || k + 1 < ke) {
+                    float2 *out = a.series + (size_t)dm * a.count * kM + (size_t)(k + rb) * kM + 1024 * h + ri;
+#pragma unroll
+                    for (int u = 0; u < 16; ++u)
+                        out[64 * u] = make_float2(yr[u] * isc, yi[u] * isc);
+                }
+            }
+            if constexpr (FOLD) {
+                float *ib = reinterpret_cast<float *>(op) + rb * kM + 1024 * h + ri;
+                const float is2 = isc * isc;
+                if (a.fold.detect) {
+#pragma unroll
+                    for (int u = 0; u < 16; ++u)
+                        ib[64 * u] = sqrtf((yr[u] * yr[u] + yi[u] * yi[u]) * is2);
+                } else {
+#pragma unroll
+                    for (int u = 0; u < 16; ++u)
+                        ib[64 * u] = (yr[u] * yr[u] + yi[u] * yi[u]) * is2;
+                }
+            }
+        };
+
+        if (np > 0) {
+            // prologue: pair 0 through GEMM 2's issue
+            unsigned char *opb = sm + kSmemOp0;
+            gather(0, opb);
             fence_proxy_async();
-            tc_fence_before();
             __syncthreads();
-            ok = true;
             if (tid == 0) {
                 tc_fence_after();
-                issue_gemm(tmem + 128, s0 + kSmemOp, s0 + kSmemBC, kIdesc2, bar);
-                ok = mbar_wait(bar, phase, kWaitLimitNs);
+                issue_cgemm(tmem, s0 + kSmemOp0, s0 + kSmemB1, 64, barA);
             }
-            phase ^= 1;
-            if (__syncthreads_or(!ok)) {
-                failed = true;
-                break;
-            }
-            tc_fence_after();
-            // ---- outputs m = M + 64 c + m2 (c = 16 h + i): series, detection
-            {
-                float yr[16], yi[16];
-                tmem_ld_2x16(tD2 + 16 * h, tD2 + 32 + 16 * h, yr, yi);
-                float *ib = rb ? ibuf1 : ibuf0;
-                const bool valid = rb == 0 || two;
-                const float is2 = isc * isc;
-#pragma unroll
-                for (int i = 0; i < 16; ++i) {
-                    const int t = 64 * (16 * h + i) + ri;
-                    if constexpr (SERIES) {
-                        if (valid)
-                            a.series[(size_t)dm * a.count * kM + (size_t)(k + rb) * kM + t] =
-                                make_float2(yr[i] * isc, yi[i] * isc);
-                    }
-                    if constexpr (FOLD) {
-                        const float pw = (yr[i] * yr[i] + yi[i] * yi[i]) * is2;
-                        ib[ipad(t)] = a.fold.detect ? sqrtf(pw) : pw;
-                    }
-                }
-            }
-            tc_fence_before();
-            if constexpr (FOLD) {
+            pendA = true;
+            failed = !wait_gemm(tid, barA, phA);
+            if (!failed) {
+                pendA = false;
+                twiddle(opb);
+                fence_proxy_async();
+                tc_fence_before();
                 __syncthreads();
-                fold_block(a.fold, fw, ibuf0, k * kM, kM, sp, sbase, scnt);
-                if (two) {
-                    __syncthreads();
-                    fold_block(a.fold, fw, ibuf1, (k + 1) * kM, kM, sp, sbase, scnt);
+                if (tid == 0) {
+                    tc_fence_after();
+                    issue_cgemm(tmem + 128, s0 + kSmemOp0, s0 + kSmemB2, 32, barB);
                 }
-                __syncthreads();  // fold reads done before the next gather overwrites them
+                pendB = true;
+            }
+            for (int i = 0; i < np && !failed; ++i) {
+                const uint32_t cur = (i & 1) ? kSmemOp1 : kSmemOp0, nxt = (i & 1) ? kSmemOp0 : kSmemOp1;
+                const bool more = i + 1 < np;
+                if (more) {
+                    // pair i + 1 into the other buffer; its GEMM 1 overlaps
+                    // pair i's outputs and fold
+                    gather(i + 1, sm + nxt);
+                    fence_proxy_async();
+                    __syncthreads();
+                    if (tid == 0) {
+                        tc_fence_after();
+                        issue_cgemm(tmem, s0 + nxt, s0 + kSmemB1, 64, barA);
+                    }
+                    pendA = true;
+                }
+                if (!wait_gemm(tid, barB, phB)) {
+                    failed = true;
+                    break;
+                }
+                pendB = false;
+                outputs(i, sm + cur);
+                tc_fence_before();
+                if constexpr (FOLD) {
+                    const int k = kb + 2 * i;
+                    const float *ib0 = reinterpret_cast<const float *>(sm + cur);
+                    __syncthreads();
+                    fold_block<false>(a.fold, fw, ib0, k * kM, kM, sp, sbase, scnt);
+                    if (k + 1 < ke) {
+                        __syncthreads();
+                        fold_block<false>(a.fold, fw, ib0 + kM, (k + 1) * kM, kM, sp, sbase, scnt);
+                    }
+                }
+                if (more) {
+                    if (!wait_gemm(tid, barA, phA)) {
+                        failed = true;
+                        break;
+                    }
+                    pendA = false;
+                    twiddle(sm + nxt);
+                    fence_proxy_async();
+                    tc_fence_before();
+                    __syncthreads();
+                    if (tid == 0) {
+                        tc_fence_after();
+                        issue_cgemm(tmem + 128, s0 + nxt, s0 + kSmemB2, 32, barB);
+                    }
+                    pendB = true;
+                }
             }
         }
         if (failed)
             break;
         if constexpr (FOLD) {
+            __syncthreads();
             if (a.fold.smem_prof) {
                 float *gm = a.fold.part_main + (size_t)w * a.fold.nbins;
                 float *gp = a.fold.part_pend + (size_t)w * a.fold.nbins;
@@ -467,7 +573,11 @@ __global__ void __launch_bounds__(kThreads, 2) tc_dedisp_kernel(DedispArgs a)
     }
     if (failed && tid == 0) {
         atomicExch(a.status, 1);
-        mbar_wait(bar, phase ^ 1, kWaitLimitNs);  // the GEMM the timed-out wait was for
+        // the GEMMs still outstanding get the same time to finish
+        if (pendA)
+            mbar_wait(barA, phA, kWaitLimitNs);
+        if (pendB)
+            mbar_wait(barB, phB, kWaitLimitNs);
     }
     tc_teardown(tmem, warp);
 }
@@ -484,25 +594,23 @@ __global__ void __launch_bounds__(kThreads, 1) tc_probe_kernel(int step, const u
     fill_constants(sm, tid);
     for (int e = tid; e < 128 * 128; e += kThreads) {
         const int r = e & 127, kk = e >> 7;
-        *reinterpret_cast<uint16_t *>(sm + kSmemOp + mn_off(r, kk)) = A[r * 128 + kk];
+        *reinterpret_cast<uint16_t *>(sm + kSmemOp0 + mn_off(r, kk)) = A[r * 128 + kk];
     }
     const uint32_t tmem = tc_setup(sm, s0, tid, warp);
     const uint32_t tcol = step == 1 ? 0u : 128u;
     if (tid == 0) {
         tc_fence_after();
-        issue_gemm(tmem + tcol, s0 + kSmemOp, s0 + (step == 1 ? kSmemBA : kSmemBC), step == 1 ? kIdesc1 : kIdesc2,
-                   bar);
+        issue_cgemm(tmem + tcol, s0 + kSmemOp0, s0 + (step == 1 ? kSmemB1 : kSmemB2), step == 1 ? 64 : 32, bar);
     }
-    bool ok = mbar_wait(bar, 0, kWaitLimitNs);
-    if (!ok && tid == 0)
-        atomicExch(status, 1);
-    if (__syncthreads_or(!ok)) {
-        if (tid == 0)
+    uint32_t parity = 0;
+    if (!wait_gemm(tid, bar, parity)) {
+        if (tid == 0) {
+            atomicExch(status, 1);
             mbar_wait(bar, 0, kWaitLimitNs);
+        }
         tc_teardown(tmem, warp);
         return;
     }
-    tc_fence_after();
     const int ncol = step == 1 ? 128 : 64;
     const int row = 32 * (warp & 3) + lane, h = warp >> 2;
     const uint32_t base = tmem + tcol + ((uint32_t)(32 * (warp & 3)) << 16);
@@ -571,7 +679,8 @@ cudaError_t launch_tc_dedisp(bool series, bool fold, const DedispArgs &a, int gr
 {
     if (!a.status)
         return cudaErrorInvalidValue;
-    const size_t sm = tc_smem_bytes(fold ? fold_smem_bytes(a.fold.nbins, a.fold.span_cap, a.fold.smem_prof != 0) : 0);
+    const size_t sm =
+        tc_smem_bytes(fold ? fold_smem_bytes(a.fold.nbins, a.fold.span_cap, a.fold.smem_prof != 0, kThreads) : 0);
     // at most two CTAs per SM (tensor memory: 256 of 512 columns each)
     if (sm * 3 <= 228u * 1024u)
         return cudaErrorInvalidConfiguration;
