@@ -9,6 +9,13 @@ FFT 4096 (MS-OSM, per-bin block delays), |y|^2 detection and folding into
 1024 phase bins per trial, all through libmsosm_b200.so.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference|reference-gpu]
+                    [--precision fp16|fp32]
+
+The headline arm (default --precision fp16) runs the inverse transforms on
+the tensor cores (tcgen05 f16 GEMMs, f32 accumulation); the plain fused FP32
+kernel is timed beside it on the same workload (`fp32_path`), and both
+paths' errors against the FP64 oracle are measured on a sample of the
+workload (`accuracy_vs_fp64`, in the CPU-baseline leg).
 
 `value`: device time (CUDA events) with the input resident in HBM.  `e2e`:
 the same metric through the C ABI with pinned HOST input, the host->device
@@ -137,6 +144,17 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+class _NoClock:
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        return False
+
+    def summary(self):
+        return None
+
+
 # ---------------------------------------------------------------------------
 # CPU baseline: the oracle on the host cores
 # ---------------------------------------------------------------------------
@@ -172,6 +190,51 @@ def cpu_baseline(dms, x, budget_s=12.0):
     return {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
             "sample": f"{len(dms)} trials x {calls * blk} samples ({calls} calls of {blk}), FP64 oracle "
                       f"(oracle/orc.c, radix-2 FFT, OpenMP over trials) incl. |y|^2 fold, {el:.1f} s"}
+
+
+def accuracy_vs_fp64(dms, x, calls=48, count=8):
+    """Relative RMS error of both device paths against the FP64 oracle on a
+    sample of the workload (the oracle is the checker here): per trial, the
+    dedispersed series and the folded |y|^2 profile."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from msosm_gpu_b200 import Dedisperser
+    O.lib().orc_set_threads(os.cpu_count() or 1)
+    o = O.Dedisp(BW, dms, F0, FFTPOINT, count, threads=os.cpu_count() or 1)
+    blk = count * o.M
+    nd = int(max(o.Nd))
+    devs = {}
+    for prec in ("fp16", "fp32"):
+        dv = Dedisperser(BW, dms, F0, FFTPOINT, count=count, precision=prec)
+        dv.fold_init(PULSAR["period"], BW, time_bin=NBINS, discard_Nd=nd, detect="power")
+        devs[prec] = dv
+    folds = [O.Fold(PULSAR["period"], BW, blk, NBINS) for _ in dms]
+    for f in folds:
+        f.discard_samples(nd)
+    err = {p: np.zeros(len(dms)) for p in devs}
+    ref = np.zeros(len(dms))
+    for c in range(calls):
+        seg = np.ascontiguousarray(x[c * blk:(c + 1) * blk])
+        y = o.filter(seg.astype(np.complex128))
+        ref += np.sum(np.abs(y) ** 2, axis=1)
+        for i, f in enumerate(folds):
+            f.fold_data(np.abs(y[i]) ** 2)
+        for p, dv in devs.items():
+            dv.filter_block(seg)
+            err[p] += np.sum(np.abs(dv.get_output().astype(np.complex128) - y) ** 2, axis=1)
+    pref = np.stack([f.fold_data_bins() for f in folds])
+    out = {"sample": f"{len(dms)} trials x {calls * blk} samples ({calls} calls of {blk}) of the workload's "
+                     f"signal; FP64 oracle (oracle/orc.c) as the reference; relative RMS per trial, "
+                     f"median and max over trials; profiles folded to {NBINS} bins after discarding {nd} samples"}
+    for p, dv in devs.items():
+        se = np.sqrt(err[p] / np.maximum(ref, 1e-300))
+        prof = dv.get_profiles().astype(np.float64)
+        pe = np.sqrt(np.sum((prof - pref) ** 2, axis=1) / np.maximum(np.sum(pref ** 2, axis=1), 1e-300))
+        out[p] = {"series_rel_rms_median": float(np.median(se)), "series_rel_rms_max": float(se.max()),
+                  "profile_rel_rms_median": float(np.median(pe)), "profile_rel_rms_max": float(pe.max()),
+                  "folded_periods": int(dv.folded_periods())}
+        dv.close()
+    return out
 
 
 # ---------------------------------------------------------------------------
@@ -223,43 +286,51 @@ def run_ours(args):
 
     # ---- value: input resident in HBM, one call per step -----------------
     blocks = samples // (FFTPOINT // 2)
-    stream = torch.cuda.Stream(dev)
-    d = Dedisperser(BW, dms, F0, FFTPOINT, count=blocks, series=False, precision=args.precision)
-    d.set_stream(stream)
-    nd_max = int(d.Nd.max())
-    d.fold_init(PULSAR["period"], BW, time_bin=NBINS, discard_Nd=nd_max, detect="power")
     xd = torch.from_numpy(x).to(dev)
-    torch.cuda.synchronize()
-    for _ in range(args.warmup):
-        d.filter_block(xd)
-    torch.cuda.synchronize()
-    d.enable_timing(True)
     uuid = None
     try:
         uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
     except Exception:
         pass
-    if ws > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    with ClockSampler(uuid) as clk:
-        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        with torch.cuda.stream(stream):
-            s.record(stream)
-            for _ in range(args.steps):
-                d.filter_block(xd)
-            e.record(stream)
-        torch.cuda.synchronize()
-    if ws > 1:
-        dist.barrier()
-    ms = s.elapsed_time(e) / args.steps
-    tm = d.timing()
     from msosm_gpu_b200 import shard
-    ms_max = shard.max_over_ranks(ms, dev)
+
+    def device_arm(precision, sample_clocks):
+        stream = torch.cuda.Stream(dev)
+        d = Dedisperser(BW, dms, F0, FFTPOINT, count=blocks, series=False, precision=precision)
+        d.set_stream(stream)
+        d.fold_init(PULSAR["period"], BW, time_bin=NBINS, discard_Nd=int(d.Nd.max()), detect="power")
+        torch.cuda.synchronize()
+        for _ in range(args.warmup):
+            d.filter_block(xd)
+        torch.cuda.synchronize()
+        d.enable_timing(True)
+        if ws > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        with ClockSampler(uuid) if sample_clocks else _NoClock() as ck:
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(stream):
+                s.record(stream)
+                for _ in range(args.steps):
+                    d.filter_block(xd)
+                e.record(stream)
+            torch.cuda.synchronize()
+        if ws > 1:
+            dist.barrier()
+        ms_max = shard.max_over_ranks(s.elapsed_time(e) / args.steps, dev)
+        tm = d.timing()
+        prof = d.get_profiles()
+        nd = int(d.Nd.max())
+        d.close()
+        return ms_max, tm, prof, ck.summary(), nd
+
     units = float(args.dms) * samples * ws
+    ms_max, tm, prof, clocks, nd_max = device_arm(args.precision, True)
     value = units / (ms_max * 1e-3) / 1e6
-    prof = d.get_profiles()
     peak_dm = float(dms[int(np.argmax(prof.max(1) - np.median(prof, 1)))])
+    other = "fp32" if args.precision == "fp16" else "fp16"
+    ms_o, tm_o, _, _, _ = device_arm(other, False)
+    value_other = units / (ms_o * 1e-3) / 1e6
 
     # ---- e2e: pinned host input through the C ABI, chunked calls -----------
     e_count = min(blocks, 4096)
@@ -286,26 +357,53 @@ def run_ours(args):
     e2e_s = (time.perf_counter() - t0) / args.steps
     e2e_v = units / shard.max_over_ranks(e2e_s, dev) / 1e6
 
-    # ---- roofline of the dominant kernel (dedisp_kernel) -------------------
+    # ---- roofline of the dominant kernel -----------------------------------
     log2n = int(math.log2(FFTPOINT))
     flops_per_sample = 10 * log2n + 16
     launch_samples = float(args.dms) * samples
-    dedisp_ms = tm["dedisp_ms"] / max(tm["calls"], 1)
-    achieved = flops_per_sample * launch_samples / (dedisp_ms * 1e-3) / 1e12
-    traffic = None
-    tr = load_traffic()
-    if tr and tr.get("bytes_per_dm_sample"):
-        traffic = tr["bytes_per_dm_sample"] * launch_samples
-    roofline = {"bound": "fp32", "achieved": achieved, "peak": fp32, "unit": "TFLOP/s",
-                "frac": achieved / fp32 if fp32 else None, "traffic": traffic,
-                "kernel": f"dedisp_kernel<{log2n}> (gather x H, inverse FFT, discard, |y|^2, fold)",
-                "flops_per_dm_sample": flops_per_sample,
-                "kernel_ms": dedisp_ms,
-                "peak_source": "cuBLAS SGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP32 "
-                               "figure; its bf16 tensor peak does not apply to an FP32 FFT)",
-                "stage_ms_per_step": {"forward": tm["forward_ms"] / max(tm["calls"], 1),
-                                      "dedisp": dedisp_ms,
-                                      "fold": tm["fold_ms"] / max(tm["calls"], 1)}}
+
+    def stages(t):
+        c = max(t["calls"], 1)
+        return {"forward": t["forward_ms"] / c, "dedisp": t["dedisp_ms"] / c, "fold": t["fold_ms"] / c}
+
+    def fp32_roofline(t):
+        k_ms = t["dedisp_ms"] / max(t["calls"], 1)
+        ach = flops_per_sample * launch_samples / (k_ms * 1e-3) / 1e12
+        return {"bound": "fp32", "achieved": ach, "peak": fp32, "unit": "TFLOP/s",
+                "frac": ach / fp32 if fp32 else None,
+                "kernel": f"dedisp_kernel<{log2n}> (gather x H, FP32 shared-memory inverse FFT, discard, |y|^2, fold)",
+                "flops_per_dm_sample": flops_per_sample, "kernel_ms": k_ms,
+                "peak_source": "cuBLAS SGEMM 8192^3 measured in this run (MEASURED_PEAKS.json has no FP32 figure)",
+                "stage_ms_per_step": stages(t)}
+
+    tr = load_traffic() or {}
+
+    def traffic_of(key):
+        b = tr.get(key)
+        return b * launch_samples if b else None
+
+    if args.precision == "fp16":
+        k_ms = tm["dedisp_ms"] / max(tm["calls"], 1)
+        tpeak = peaks.get("bf16_tflops_sustained") or 1374.0
+        ach = flops_per_sample * launch_samples / (k_ms * 1e-3) / 1e12
+        # executed tensor work: per pair of 4096-point blocks 128x128x128 + 128x64x128 MACs
+        exec_tf = 2.0 * (128 * 128 * 128 + 128 * 64 * 128) / 4096.0 * launch_samples / (k_ms * 1e-3) / 1e12
+        roofline = {"bound": "tensor", "achieved": ach, "peak": tpeak, "unit": "TFLOP/s", "frac": ach / tpeak,
+                    "traffic": traffic_of("tc_bytes_per_dm_sample"),
+                    "kernel": "tc_dedisp_kernel (gather x H, inverse FFT as two tcgen05 f16 GEMMs + f16 twiddle, "
+                              "discard, |y|^2, fold)",
+                    "flops_per_dm_sample": flops_per_sample, "kernel_ms": k_ms,
+                    "executed_tensor_tflops": exec_tf, "executed_tensor_frac": exec_tf / tpeak,
+                    "peak_source": "MEASURED_PEAKS.json bf16_tflops_sustained (f16 runs at the bf16 rate; the "
+                                   "kernel runs inside a ~100 ms step)",
+                    "note": "achieved counts the algorithmic 10 log2 N + 16 flops per DM-trial sample, as the "
+                            "FP32 path does; the kernel is bound by CUDA-core issue (gather, twiddle, fold), "
+                            "not by the tensor pipe",
+                    "stage_ms_per_step": stages(tm)}
+        roofline_fp32 = dict(fp32_roofline(tm_o), traffic=traffic_of("bytes_per_dm_sample"))
+    else:
+        roofline = dict(fp32_roofline(tm), traffic=traffic_of("bytes_per_dm_sample"))
+        roofline_fp32 = None
     hbm = peaks.get("hbm_gbs")
     algo_bytes = 8.0 * samples  # the input, read once for all trials
     roofline_hbm = {"bound": "hbm", "algorithmic_bytes_per_step": algo_bytes,
@@ -314,18 +412,25 @@ def run_ours(args):
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded pulsar + AWGN)",
-            "config": workload_config(samples, args.dms, ws),
+            "vs_baseline": None,
+            "dtype": "f16 GEMM operands, f32 accumulation and gather" if args.precision == "fp16" else "f32",
+            "data": "synthetic (seeded pulsar + AWGN)",
+            "config": dict(workload_config(samples, args.dms, ws), precision=args.precision),
             "e2e": {"value": e2e_v, "unit": UNIT, "h2d_bytes_per_step": int(x.nbytes),
                     "d2h_bytes_per_step": int(prof.nbytes), "ms_per_step": e2e_s * 1e3,
                     "calls_per_step": calls},
             "gpu_launches": int(tm["kernel_launches"]),
             "roofline": roofline, "roofline_hbm": roofline_hbm,
-            "clocks": clk.summary(),
+            "clocks": clocks,
+            other + "_path": {"value": value_other, "ms_per_step": ms_o, "unit": UNIT,
+                              "note": "the same workload through the other precision's fused kernel, timed "
+                                      "the same way (value / this = %.3f)" % (value / value_other)},
             "check": {"detected_dm": peak_dm, "injected_dm": PULSAR["dm"]}}
+    if roofline_fp32:
+        line["roofline_fp32_path"] = roofline_fp32
     if rank == 0 and ws == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(dms, x)
-    d.close()
+        line["accuracy_vs_fp64"] = accuracy_vs_fp64(dms, x)
     de.close()
     if ws > 1:
         dist.barrier()
@@ -413,7 +518,7 @@ def main():
     ap.add_argument("--log2-samples", type=int, default=LOG2_SAMPLES)
     ap.add_argument("--dms", type=int, default=N_DM)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp16"],
+    ap.add_argument("--precision", default="fp16", choices=["fp32", "fp16"],
                     help="inverse transforms on the CUDA cores (fp32) or the tensor cores (fp16)")
     args = ap.parse_args()
     if args.impl == "reference":
