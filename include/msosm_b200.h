@@ -285,6 +285,48 @@ MSOSM_API msosm_status msosm_fold_planner_chunk(msosm_fold_planner *p, unsigned 
                                       unsigned long long *completed);
 
 /* ======================================================================
+ * PSRDADA baseband files (host I/O)
+ * ====================================================================== */
+
+/* A 4096-byte ASCII header of "KEY value" lines, then frames of 2048
+ * uint16 pairs of polarisation 1 followed by 2048 of polarisation 2.
+ * Replaces the PSRDADA class (psrdada/psrdada.cpp:3-94,
+ * psrdada/include/psrdada.h:11-43).  Keys are read as the reference reads
+ * them: a line splits at its first space, the value starts at the next
+ * non-space character; fields whose key is absent stay 0 (the reference
+ * leaves them uninitialised). */
+typedef struct msosm_dada msosm_dada;
+#define MSOSM_DADA_HAVE_BW 0x1u   /* BW was present */
+#define MSOSM_DADA_HAVE_FREQ 0x2u /* FREQ was present */
+typedef struct msosm_dada_info {
+    float bw;   /* BW, MHz */
+    float fc;   /* FREQ (centre), MHz */
+    int nbit;
+    int nchan;
+    int ndim;
+    int npol;
+    unsigned int have;              /* MSOSM_DADA_HAVE_* */
+    unsigned long long filesize;    /* bytes, header included */
+} msosm_dada_info;
+
+/* Open and parse the header (PSRDADA::PSRDADA, psrdada.cpp:3-50). */
+MSOSM_API msosm_status msosm_dada_open(const char *path, msosm_dada **out);
+MSOSM_API msosm_status msosm_dada_close(msosm_dada *d);
+MSOSM_API msosm_status msosm_dada_get_info(const msosm_dada *d, msosm_dada_info *info);
+/* The raw 4096 header bytes (PSRDADA::headerBuffer). */
+MSOSM_API msosm_status msosm_dada_get_header(const msosm_dada *d, char *header4096);
+/* Whole reads of n samples per polarisation the file holds:
+ * (filesize - 4096) / (2 n 4) (PSRDADA::initBuffer's readCount,
+ * psrdada.cpp:57-78).  n: a positive multiple of 2048. */
+MSOSM_API msosm_status msosm_dada_read_count(const msosm_dada *d, unsigned long n, unsigned long *count);
+/* The next n samples of each polarisation, de-interleaved frame by frame
+ * into pol1 and pol2 (host buffers of n pairs each; PSRDADA::readSamples,
+ * psrdada.cpp:80-87).  Returns MSOSM_ERR_STATE, reading nothing, when fewer
+ * than 2n samples are left (the reference reads past the end silently). */
+MSOSM_API msosm_status msosm_dada_read(msosm_dada *d, unsigned long n, msosm_uint16_pair *pol1,
+                                       msosm_uint16_pair *pol2);
+
+/* ======================================================================
  * Diagnostics (no counterpart in the reference)
  * ====================================================================== */
 

@@ -496,4 +496,68 @@ private:
     std::vector<float> folded_, intensity_;
 };
 
+// ---------------------------------------------------------------------------
+// psrdada/include/psrdada.h:17-43 -- a PSRDADA file (msosm_dada_*)
+// ---------------------------------------------------------------------------
+
+class PSRDADA {
+public:
+    explicit PSRDADA(std::string filename) : infileName(std::move(filename))
+    {
+        check(msosm_dada_open(infileName.c_str(), &h_), "PSRDADA");
+        msosm_dada_info info;
+        check(msosm_dada_get_info(h_, &info), "PSRDADA");
+        check(msosm_dada_get_header(h_, headerBuffer), "PSRDADA");
+        filesize = (unsigned long)info.filesize;
+        bw = info.bw;
+        fc = info.fc;
+        nbit = info.nbit;
+        nchan = info.nchan;
+        ndim = info.ndim;
+        npol = info.npol;
+        outfileName = infileName.substr(0, infileName.find_last_of('.')) + "_dedisp_folded.txt";
+        std::printf("%g %g %d %d %d %d\n", bw, fc, nbit, nchan, ndim, npol);
+    }
+    PSRDADA(const PSRDADA &) = delete;
+    PSRDADA &operator=(const PSRDADA &) = delete;
+    ~PSRDADA()
+    {
+        if (h_)
+            msosm_dada_close(h_);
+    }
+    // n: samples per polarisation and read, a multiple of 2048
+    void initBuffer(size_t n)
+    {
+        if (n % 2048 != 0)
+            check(MSOSM_ERR_BAD_ARG, "initBuffer: n must be a multiple of frameSamples (2048)");
+        pol1_.assign(n, uint16_pair{0, 0});
+        pol2_.assign(n, uint16_pair{0, 0});
+        pol1_in = pol1_.data();
+        pol2_in = pol2_.data();
+        frameCount = (int)(n / 2048);
+        check(msosm_dada_read_count(h_, n, &readCount), "initBuffer");
+    }
+    void readSamples() { check(msosm_dada_read(h_, pol1_.size(), pol1_in, pol2_in), "readSamples"); }
+
+    char headerBuffer[4096] = {0};
+    std::string infileName;
+    unsigned long filesize = 0;
+    unsigned long readCount = 0;
+    std::string outfileName;
+    float bw = 0.f;
+    float fc = 0.f;
+    int nbit = 0;
+    int nchan = 0;
+    int ndim = 0;
+    int npol = 0;
+    int hdr_size = 4096;
+    uint16_pair *pol1_in = nullptr;
+    uint16_pair *pol2_in = nullptr;
+    int frameCount = 0;
+
+private:
+    msosm_dada *h_ = nullptr;
+    std::vector<uint16_pair> pol1_, pol2_;
+};
+
 }  // namespace msosm_b200

@@ -111,6 +111,12 @@ def _declare(L: ctypes.CDLL) -> None:
         "msosm_fold_planner_destroy": (i32, [vp]),
         "msosm_fold_planner_chunk": (i32, [vp, ul, vp, pull]),
         "msosm_tc_gemm_check": (i32, [i32, vp, vp]),
+        "msosm_dada_open": (i32, [ctypes.c_char_p, pvp]),
+        "msosm_dada_close": (i32, [vp]),
+        "msosm_dada_get_info": (i32, [vp, vp]),
+        "msosm_dada_get_header": (i32, [vp, vp]),
+        "msosm_dada_read_count": (i32, [vp, ul, pul]),
+        "msosm_dada_read": (i32, [vp, ul, vp, vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

@@ -19,6 +19,7 @@
 #include "prepare_concurrent.h"
 #include "fold_gpu.h"
 #include "simulated_complex_signal.h"
+#include "psrdada.h"
 
 namespace {
 
@@ -45,7 +46,8 @@ int usage()
                  "ref_golden concurrent <bw> <f0> <fftpoint> <out> <dm...>\n"
                  "ref_golden osm <bw> <dm> <f0> <fftpoint> <out>\n"
                  "ref_golden fold <period> <fs> <size> <time_bin|-1> <Nd|-1> <nchunks> <in.f32> <out>\n"
-                 "ref_golden simulate <bw> <dm> <f0> <period> <repeat> <out>\n");
+                 "ref_golden simulate <bw> <dm> <f0> <period> <repeat> <out>\n"
+                 "ref_golden dada <file> <n> <reads> <out>\n");
     return 2;
 }
 
@@ -174,6 +176,28 @@ int main(int argc, char **argv)
         rec_u64("Nd", s.Nd);
         rec("signal", "f4", s.signal, 2 * s.signal_size, 4);
         rec("signal_u16", "u2", s.signal_u16, 2 * s.signal_size, 2);
+    } else if (mode == "dada" && argc == 6) {
+        // PSRDADA::PSRDADA + initBuffer + readSamples (psrdada/psrdada.cpp:3-94)
+        unsigned long n = std::strtoul(argv[3], nullptr, 10);
+        int reads = std::atoi(argv[4]);
+        g_out = std::fopen(argv[5], "wb");
+        PSRDADA file(argv[2]);
+        file.initBuffer(n);
+        float f[2] = {file.bw, file.fc};
+        int32_t i[4] = {file.nbit, file.nchan, file.ndim, file.npol};
+        rec("bw_fc", "f4", f, 2, 4);
+        rec("nbit_nchan_ndim_npol", "i4", i, 4, 4);
+        rec_u64("filesize", file.filesize);
+        rec_u64("readCount", file.readCount);
+        rec_u64("frameCount", (uint64_t)file.frameCount);
+        std::vector<uint16_pair> p1, p2;
+        for (int r = 0; r < reads; r++) {
+            file.readSamples();
+            p1.insert(p1.end(), file.pol1_in, file.pol1_in + n);
+            p2.insert(p2.end(), file.pol2_in, file.pol2_in + n);
+        }
+        rec("pol1", "u2", p1.data(), 2 * p1.size(), 2);
+        rec("pol2", "u2", p2.data(), 2 * p2.size(), 2);
     } else {
         return usage();
     }
