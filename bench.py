@@ -204,7 +204,7 @@ def accuracy_vs_fp64(dms, x, calls=48, count=8):
     blk = count * o.M
     nd = int(max(o.Nd))
     devs = {}
-    for prec in ("fp16", "fp32"):
+    for prec in ("fp16", "bf16", "fp32"):
         dv = Dedisperser(BW, dms, F0, FFTPOINT, count=count, precision=prec)
         dv.fold_init(PULSAR["period"], BW, time_bin=NBINS, discard_Nd=nd, detect="power")
         devs[prec] = dv

@@ -129,6 +129,9 @@ typedef struct msosm_dedisp msosm_dedisp;
  * sizes return MSOSM_ERR_UNSUPPORTED).  Relative RMS error of the series
  * against FP64: about 5e-4; folded profiles much lower. */
 #define MSOSM_FLAG_TENSOR_F16 0x4u
+/* As MSOSM_FLAG_TENSOR_F16 with bf16 operands (no scaling needed; relative
+ * RMS error of the series against FP64 about 4e-3). */
+#define MSOSM_FLAG_TENSOR_BF16 0x8u
 
 typedef struct msosm_dedisp_info {
     unsigned long M;        /* hop / filter order; FFT size is 2M */

@@ -45,7 +45,10 @@ inline unsigned int &extra_flags()
     static unsigned int f = 0;
     return f;
 }
-inline void use_tensor_cores(bool on) { extra_flags() = on ? MSOSM_FLAG_TENSOR_F16 : 0u; }
+inline void use_tensor_cores(bool on, bool bf16 = false)
+{
+    extra_flags() = on ? (bf16 ? MSOSM_FLAG_TENSOR_BF16 : MSOSM_FLAG_TENSOR_F16) : 0u;
+}
 
 inline void check(msosm_status s, const char *what)
 {

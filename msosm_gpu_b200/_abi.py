@@ -25,6 +25,7 @@ ERR_NO_DEVICE = 7
 FLAG_OSM = 0x1
 FLAG_NO_SERIES = 0x2
 FLAG_TENSOR_F16 = 0x4
+FLAG_TENSOR_BF16 = 0x8
 DETECT_POWER = 0
 DETECT_AMPLITUDE = 1
 

@@ -133,7 +133,7 @@ struct msosm_dedisp {
     // inverse transforms on the tensor cores (MSOSM_FLAG_TENSOR_F16): ring,
     // H and delays in tensor-core order (tc_layout.hpp); status_d != 0 after
     // a timed-out wait in the kernel
-    bool tc = false;
+    bool tc = false, tc_bf16 = false;
     int *status_d = nullptr;
     float *row_max = nullptr;  // [S] largest |component| of each ring row
     float *h_max = nullptr;    // [D] largest |component| of each trial's H
@@ -241,7 +241,7 @@ cudaError_t plan_grid(msosm_dedisp *d)
         return e;
     const int threads = d->tc ? tc::kThreads : (int)(d->N / 16);
     const size_t extra = d->fold ? fold_smem_bytes(d->nbins, d->win_cap, d->nbins <= kMaxSmemBins, threads) : 0;
-    int per_sm = d->tc ? tc_blocks_per_sm(d->series, d->fold, extra)
+    int per_sm = d->tc ? tc_blocks_per_sm(d->tc_bf16, d->series, d->fold, extra)
                        : dedisp_blocks_per_sm(d->log2n, d->pingpong, d->series, d->fold, extra);
     if (per_sm < 1)
         per_sm = 1;
@@ -480,7 +480,7 @@ msosm_status msosm_dedisp_create(const float *bw, const float *dm, const float *
     if (!out || !bw || !dm || !f0 || numDMs < 1)
         return fail(MSOSM_ERR_BAD_ARG, "msosm_dedisp_create: null argument or numDMs < 1");
     *out = nullptr;
-    if (flags & ~(MSOSM_FLAG_OSM | MSOSM_FLAG_NO_SERIES | MSOSM_FLAG_TENSOR_F16))
+    if (flags & ~(MSOSM_FLAG_OSM | MSOSM_FLAG_NO_SERIES | MSOSM_FLAG_TENSOR_F16 | MSOSM_FLAG_TENSOR_BF16))
         return fail(MSOSM_ERR_BAD_ARG, "unknown flags 0x%x", flags);
     for (int i = 0; i < numDMs; ++i)
         if (!(bw[i] > 0) || !(f0[i] > 0) || !(dm[i] >= 0) || !std::isfinite(dm[i]))
@@ -519,10 +519,15 @@ msosm_status msosm_dedisp_create(const float *bw, const float *dm, const float *
         return fail(MSOSM_ERR_UNSUPPORTED, "FFT size %lu outside the supported 64..2^24", 2 * M);
     }
     d->large = !log2n_supported(log2n);
-    d->tc = (flags & MSOSM_FLAG_TENSOR_F16) != 0;
+    d->tc = (flags & (MSOSM_FLAG_TENSOR_F16 | MSOSM_FLAG_TENSOR_BF16)) != 0;
+    d->tc_bf16 = (flags & MSOSM_FLAG_TENSOR_BF16) != 0;
+    if ((flags & MSOSM_FLAG_TENSOR_F16) && d->tc_bf16) {
+        release(d);
+        return fail(MSOSM_ERR_BAD_ARG, "MSOSM_FLAG_TENSOR_F16 and MSOSM_FLAG_TENSOR_BF16 exclude each other");
+    }
     if (d->tc && !tc_supported(log2n)) {
         release(d);
-        return fail(MSOSM_ERR_UNSUPPORTED, "MSOSM_FLAG_TENSOR_F16 needs FFT size %d (got %lu)", tc::kN, 2 * M);
+        return fail(MSOSM_ERR_UNSUPPORTED, "the tensor-core path needs FFT size %d (got %lu)", tc::kN, 2 * M);
     }
     if (input_size != 0)
         count = (int)(input_size / M);
@@ -983,7 +988,7 @@ static msosm_status filter_block(msosm_dedisp *d, const void *input, InputKind k
     if (ev)
         CK(cudaEventRecord(ev->e[2], d->stream));
     if (d->tc)
-        CK(launch_tc_dedisp(d->series, d->fold, da, d->grid, d->stream));
+        CK(launch_tc_dedisp(d->tc_bf16, d->series, d->fold, da, d->grid, d->stream));
     else
         CK(launch_dedisp(d->log2n, d->pingpong, d->series, d->fold, da, d->grid, d->stream));
     d->launches += 1;

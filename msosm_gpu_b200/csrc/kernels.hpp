@@ -119,10 +119,11 @@ cudaError_t launch_fold_series(const float *I, long long n, int R, const FoldArg
 bool tc_supported(int log2n);
 // dynamic shared memory of the tensor-core kernel with `extra` fold bytes
 size_t tc_smem_bytes(size_t extra);
-int tc_blocks_per_sm(bool series, bool fold, size_t extra_smem);
+int tc_blocks_per_sm(bool bf16, bool series, bool fold, size_t extra_smem);
 // a.H and a.delays in tensor-core order (tc_layout.hpp), ring written with
 // FwdArgs::tc_order; a.R counts ranges of block pairs
-cudaError_t launch_tc_dedisp(bool series, bool fold, const DedispArgs &a, int grid, cudaStream_t st);
+// bf16: bf16 operands (else f16)
+cudaError_t launch_tc_dedisp(bool bf16, bool series, bool fold, const DedispArgs &a, int grid, cudaStream_t st);
 // rows of n bins (n = 4096) from natural into tensor-core order, in place via scratch
 cudaError_t launch_tc_permute_rows(const float2 *in, float2 *out, int rows, cudaStream_t st);
 // one GEMM of the kernel on given data: a = 128 x 128 f16 bit patterns

@@ -27,6 +27,7 @@
 // frees its tensor memory and returns.
 #include <algorithm>
 
+#include <cuda_bf16.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
@@ -144,9 +145,26 @@ __device__ __forceinline__ void tmem_ld_2x16(uint32_t ta, uint32_t tb, float (&a
     }
 }
 
-__device__ __forceinline__ uint32_t pack_half2(float lo, float hi)
+// The 16-bit operand type: f16 (scaled into range) or bf16.
+struct F16 {
+    using h1 = __half;
+    using h2 = __half2;
+    static constexpr uint32_t fmt = 0;  // instruction-descriptor A/B format
+    __device__ static h2 pack(float lo, float hi) { return __floats2half2_rn(lo, hi); }
+    __device__ static h1 one(float v) { return __float2half_rn(v); }
+};
+struct BF16 {
+    using h1 = __nv_bfloat16;
+    using h2 = __nv_bfloat162;
+    static constexpr uint32_t fmt = 1;
+    __device__ static h2 pack(float lo, float hi) { return __floats2bfloat162_rn(lo, hi); }
+    __device__ static h1 one(float v) { return __float2bfloat16_rn(v); }
+};
+
+template <class E>
+__device__ __forceinline__ uint32_t pack2(float lo, float hi)
 {
-    const __half2 h = __floats2half2_rn(lo, hi);
+    const typename E::h2 h = E::pack(lo, hi);
     return *reinterpret_cast<const uint32_t *>(&h);
 }
 
@@ -177,19 +195,20 @@ __device__ __forceinline__ float warp_max(float v)
 //     n >= 64 -> sin(2 pi k2 (n - 64) / 64)            (output frequency m2)
 //   GEMM 2, B2[n][k1], k1 < 64: n < 32 -> cos(2 pi k1 (32 + n) / 64),
 //     n >= 32 -> sin(2 pi k1 n / 64)                   (output m1 = 32..63)
+template <class E>
 __device__ void fill_constants(unsigned char *sm, int tid)
 {
     for (int e = tid; e < 128 * 64; e += kThreads) {
         const int n = e >> 6, k = e & 63;
         float s, c;
         sincospif((float)((k * (n & 63)) & 63) * (1.0f / 32.0f), &s, &c);
-        *reinterpret_cast<__half *>(sm + kSmemB1 + k_off(n, k)) = __float2half_rn(n < 64 ? c : s);
+        *reinterpret_cast<typename E::h1 *>(sm + kSmemB1 + k_off(n, k)) = E::one(n < 64 ? c : s);
     }
     for (int e = tid; e < 64 * 64; e += kThreads) {
         const int n = e >> 6, k = e & 63;
         float s, c;
         sincospif((float)((k * (32 + (n & 31))) & 63) * (1.0f / 32.0f), &s, &c);
-        *reinterpret_cast<__half *>(sm + kSmemB2 + k_off(n, k)) = __float2half_rn(n < 32 ? c : s);
+        *reinterpret_cast<typename E::h1 *>(sm + kSmemB2 + k_off(n, k)) = E::one(n < 32 ? c : s);
     }
 }
 
@@ -226,11 +245,12 @@ __device__ __forceinline__ void tc_teardown(uint32_t tmem, int warp)
 // Im] K = 128, MN-major at a) x the DFT whose [C | S] (K = 64, n2 columns)
 // is at b; then the commit to the mbarrier.  Three passes of four K = 16
 // steps: Re x [C | S], then -Im x S into the Re half, Im x C into the Im half.
+template <class E>
 __device__ __forceinline__ void issue_cgemm(uint32_t tmem_d, uint32_t a, uint32_t b, int half, uint32_t bar)
 {
-    const uint32_t id_full = idesc_f16(128, 2 * half, true);
-    const uint32_t id_neg = idesc_f16(128, half, true, true);
-    const uint32_t id_half = idesc_f16(128, half, true);
+    const uint32_t id_full = idesc_f16(128, 2 * half, true, false, E::fmt);
+    const uint32_t id_neg = idesc_f16(128, half, true, true, E::fmt);
+    const uint32_t id_half = idesc_f16(128, half, true, false, E::fmt);
 #pragma unroll
     for (int s = 0; s < 4; ++s)
         mma_f16(tmem_d, smem_desc(a + s * kDescStepA, 2048, 128), smem_desc(b + s * kDescStepB, 128, 1024),
@@ -261,7 +281,7 @@ __device__ __forceinline__ bool wait_gemm(int tid, uint32_t bar, uint32_t &parit
     return !failed;
 }
 
-template <bool SERIES, bool FOLD>
+template <class E, bool SERIES, bool FOLD>
 __global__ void __launch_bounds__(kThreads, 2) tc_dedisp_kernel(DedispArgs a)
 {
     extern __shared__ __align__(1024) unsigned char sm[];
@@ -271,7 +291,7 @@ __global__ void __launch_bounds__(kThreads, 2) tc_dedisp_kernel(DedispArgs a)
     FoldSmem fw;
     if constexpr (FOLD)
         fold_smem_layout(fw, sm + kSmemFold, a.fold);
-    fill_constants(sm, tid);
+    fill_constants<E>(sm, tid);
     const uint32_t tmem = tc_setup(sm, s0, tid, warp);
     // epilogue view: warp w reads TMEM lanes 32 (w % 4) .. + 31 (its GEMM
     // rows) and half h = w / 4 of the columns
@@ -282,15 +302,15 @@ __global__ void __launch_bounds__(kThreads, 2) tc_dedisp_kernel(DedispArgs a)
     const int rb = row >> 6, ri = row & 63;  // block of the pair; k1 (GEMM 1) / m2 (GEMM 2)
     // this thread's twiddles e^{+2 pi i ri m2 / 4096}, m2 = 32 h + i, as f16
     // pairs (m2, m2 + 1) matching the operand packing
-    __half2 twr[16], twi[16];
+    typename E::h2 twr[16], twi[16];
 #pragma unroll
     for (int i = 0; i < 16; ++i) {
         float s0f, c0f, s1f, c1f;
         const int m2 = 32 * h + 2 * i;
         sincospif((float)((ri * m2) & 4095) * (1.0f / 2048.0f), &s0f, &c0f);
         sincospif((float)((ri * (m2 + 1)) & 4095) * (1.0f / 2048.0f), &s1f, &c1f);
-        twr[i] = __floats2half2_rn(c0f, c1f);
-        twi[i] = __floats2half2_rn(s0f, s1f);
+        twr[i] = E::pack(c0f, c1f);
+        twi[i] = E::pack(s0f, s1f);
     }
 
     const float4 *__restrict__ ring4 = reinterpret_cast<const float4 *>(a.ring);
@@ -389,8 +409,8 @@ __global__ void __launch_bounds__(kThreads, 2) tc_dedisp_kernel(DedispArgs a)
                         const float zr0 = x[b].x * hv.x - x[b].y * hv.y, zi0 = x[b].x * hv.y + x[b].y * hv.x;
                         const float zr1 = x[b].z * hv.z - x[b].w * hv.w, zi1 = x[b].z * hv.w + x[b].w * hv.z;
                         const int off = (b * 8 + j) * 128 + warp * 2048 + (lane >> 2) * 16 + (lane & 3) * 4;
-                        *reinterpret_cast<uint32_t *>(op + off) = pack_half2(zr0, zr1);
-                        *reinterpret_cast<uint32_t *>(op + off + 8 * 2048) = pack_half2(zi0, zi1);
+                        *reinterpret_cast<uint32_t *>(op + off) = pack2<E>(zr0, zr1);
+                        *reinterpret_cast<uint32_t *>(op + off + 8 * 2048) = pack2<E>(zi0, zi1);
                     }
                 }
             } else {
@@ -419,8 +439,8 @@ __global__ void __launch_bounds__(kThreads, 2) tc_dedisp_kernel(DedispArgs a)
                         const float zr0 = x.x * hv.x - x.y * hv.y, zi0 = x.x * hv.y + x.y * hv.x;
                         const float zr1 = x.z * hv.z - x.w * hv.w, zi1 = x.z * hv.w + x.w * hv.z;
                         const int off = (b * 8 + j) * 128 + warp * 2048 + (lane >> 2) * 16 + (lane & 3) * 4;
-                        *reinterpret_cast<uint32_t *>(op + off) = pack_half2(zr0, zr1);
-                        *reinterpret_cast<uint32_t *>(op + off + 8 * 2048) = pack_half2(zi0, zi1);
+                        *reinterpret_cast<uint32_t *>(op + off) = pack2<E>(zr0, zr1);
+                        *reinterpret_cast<uint32_t *>(op + off + 8 * 2048) = pack2<E>(zi0, zi1);
                     }
                 }
             }
@@ -436,11 +456,11 @@ __global__ void __launch_bounds__(kThreads, 2) tc_dedisp_kernel(DedispArgs a)
                 uint32_t pr[8], pim[8];
 #pragma unroll
                 for (int i = 0; i < 8; ++i) {
-                    const __half2 ar = __floats2half2_rn(re[2 * i], re[2 * i + 1]);
-                    const __half2 ai = __floats2half2_rn(im[2 * i], im[2 * i + 1]);
-                    const __half2 wr = twr[8 * p + i], wi = twi[8 * p + i];
-                    const __half2 orr = __hfma2(ar, wr, __hneg2(__hmul2(ai, wi)));
-                    const __half2 oi = __hfma2(ar, wi, __hmul2(ai, wr));
+                    const typename E::h2 ar = E::pack(re[2 * i], re[2 * i + 1]);
+                    const typename E::h2 ai = E::pack(im[2 * i], im[2 * i + 1]);
+                    const typename E::h2 wr = twr[8 * p + i], wi = twi[8 * p + i];
+                    const typename E::h2 orr = __hfma2(ar, wr, __hneg2(__hmul2(ai, wi)));
+                    const typename E::h2 oi = __hfma2(ar, wi, __hmul2(ai, wr));
                     pr[i] = *reinterpret_cast<const uint32_t *>(&orr);
                     pim[i] = *reinterpret_cast<const uint32_t *>(&oi);
                 }
@@ -490,7 +510,7 @@ __global__ void __launch_bounds__(kThreads, 2) tc_dedisp_kernel(DedispArgs a)
             __syncthreads();
             if (tid == 0) {
                 tc_fence_after();
-                issue_cgemm(tmem, s0 + kSmemOp0, s0 + kSmemB1, 64, barA);
+                issue_cgemm<E>(tmem, s0 + kSmemOp0, s0 + kSmemB1, 64, barA);
             }
             pendA = true;
             failed = !wait_gemm(tid, barA, phA);
@@ -502,7 +522,7 @@ __global__ void __launch_bounds__(kThreads, 2) tc_dedisp_kernel(DedispArgs a)
                 __syncthreads();
                 if (tid == 0) {
                     tc_fence_after();
-                    issue_cgemm(tmem + 128, s0 + kSmemOp0, s0 + kSmemB2, 32, barB);
+                    issue_cgemm<E>(tmem + 128, s0 + kSmemOp0, s0 + kSmemB2, 32, barB);
                 }
                 pendB = true;
             }
@@ -517,7 +537,7 @@ __global__ void __launch_bounds__(kThreads, 2) tc_dedisp_kernel(DedispArgs a)
                     __syncthreads();
                     if (tid == 0) {
                         tc_fence_after();
-                        issue_cgemm(tmem, s0 + nxt, s0 + kSmemB1, 64, barA);
+                        issue_cgemm<E>(tmem, s0 + nxt, s0 + kSmemB1, 64, barA);
                     }
                     pendA = true;
                 }
@@ -550,7 +570,7 @@ __global__ void __launch_bounds__(kThreads, 2) tc_dedisp_kernel(DedispArgs a)
                     __syncthreads();
                     if (tid == 0) {
                         tc_fence_after();
-                        issue_cgemm(tmem + 128, s0 + nxt, s0 + kSmemB2, 32, barB);
+                        issue_cgemm<E>(tmem + 128, s0 + nxt, s0 + kSmemB2, 32, barB);
                     }
                     pendB = true;
                 }
@@ -591,7 +611,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_probe_kernel(int step, const u
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t s0 = smem_addr(sm);
     const uint32_t bar = s0 + kSmemCtl;
-    fill_constants(sm, tid);
+    fill_constants<F16>(sm, tid);
     for (int e = tid; e < 128 * 128; e += kThreads) {
         const int r = e & 127, kk = e >> 7;
         *reinterpret_cast<uint16_t *>(sm + kSmemOp0 + mn_off(r, kk)) = A[r * 128 + kk];
@@ -600,7 +620,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_probe_kernel(int step, const u
     const uint32_t tcol = step == 1 ? 0u : 128u;
     if (tid == 0) {
         tc_fence_after();
-        issue_cgemm(tmem + tcol, s0 + kSmemOp0, s0 + (step == 1 ? kSmemB1 : kSmemB2), step == 1 ? 64 : 32, bar);
+        issue_cgemm<F16>(tmem + tcol, s0 + kSmemOp0, s0 + (step == 1 ? kSmemB1 : kSmemB2), step == 1 ? 64 : 32, bar);
     }
     uint32_t parity = 0;
     if (!wait_gemm(tid, bar, parity)) {
@@ -632,17 +652,25 @@ __global__ void tc_permute_kernel(const float2 *__restrict__ in, float2 *__restr
         out[(i & ~(long long)(kN - 1)) + tc_pos((int)(i & (kN - 1)))] = in[i];
 }
 
-template <bool SERIES, bool FOLD>
-auto tc_fn() { return tc_dedisp_kernel<SERIES, FOLD>; }
+template <class E, bool SERIES, bool FOLD>
+auto tc_fn() { return tc_dedisp_kernel<E, SERIES, FOLD>; }
 
-template <typename G>
-auto tc_select(bool series, bool fold, G &&go)
+template <class E, typename G>
+auto tc_select_e(bool series, bool fold, G &&go)
 {
     if (series && fold)
-        return go(tc_fn<true, true>());
+        return go(tc_fn<E, true, true>());
     if (fold)
-        return go(tc_fn<false, true>());
-    return go(tc_fn<true, false>());
+        return go(tc_fn<E, false, true>());
+    return go(tc_fn<E, true, false>());
+}
+
+template <typename G>
+auto tc_select(bool bf16, bool series, bool fold, G &&go)
+{
+    if (bf16)
+        return tc_select_e<BF16>(series, fold, go);
+    return tc_select_e<F16>(series, fold, go);
 }
 
 }  // namespace
@@ -655,7 +683,7 @@ size_t tc_smem_bytes(size_t extra) { return (size_t)kSmemFold + extra; }
 // two: each CTA holds 256 of the SM's 512 tensor-memory columns).  The
 // occupancy API is not used here: it reports one CTA per SM for this kernel
 // where the hardware runs two.
-int tc_blocks_per_sm(bool series, bool fold, size_t extra_smem)
+int tc_blocks_per_sm(bool bf16, bool series, bool fold, size_t extra_smem)
 {
     const size_t sm = tc_smem_bytes(extra_smem);
     int dev = 0, smem_sm = 0, reserved = 0, regs_sm = 0;
@@ -664,7 +692,7 @@ int tc_blocks_per_sm(bool series, bool fold, size_t extra_smem)
         cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev) != cudaSuccess)
         return 0;
-    return tc_select(series, fold, [&](auto k) -> int {
+    return tc_select(bf16, series, fold, [&](auto k) -> int {
         cudaFuncAttributes fa;
         if (cudaFuncGetAttributes(&fa, k) != cudaSuccess)
             return 0;
@@ -675,7 +703,7 @@ int tc_blocks_per_sm(bool series, bool fold, size_t extra_smem)
     });
 }
 
-cudaError_t launch_tc_dedisp(bool series, bool fold, const DedispArgs &a, int grid, cudaStream_t st)
+cudaError_t launch_tc_dedisp(bool bf16, bool series, bool fold, const DedispArgs &a, int grid, cudaStream_t st)
 {
     if (!a.status)
         return cudaErrorInvalidValue;
@@ -684,7 +712,7 @@ cudaError_t launch_tc_dedisp(bool series, bool fold, const DedispArgs &a, int gr
     // at most two CTAs per SM (tensor memory: 256 of 512 columns each)
     if (sm * 3 <= 228u * 1024u)
         return cudaErrorInvalidConfiguration;
-    return tc_select(series, fold, [&](auto k) -> cudaError_t {
+    return tc_select(bf16, series, fold, [&](auto k) -> cudaError_t {
         cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e == cudaSuccess)
             e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,

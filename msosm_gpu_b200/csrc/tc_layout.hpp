@@ -81,13 +81,15 @@ constexpr uint32_t kDescStepA = 2 * 2048;  // MN-major data operand (LBO 2048, S
 constexpr uint32_t kDescStepB = 2 * 128;   // K-major constant operand (LBO 128, SBO 1024)
 __host__ __device__ constexpr uint32_t b_col(int n) { return (uint32_t)(n >> 3) * 1024; }
 
-// Instruction descriptor, kind::f16: f32 accumulator (bits 4-5 = 1), f16 A
-// and B (bits 7-9, 10-12 = 0), negate A (bit 13), A MN-major (bit 15), B
-// K-major (bit 16 = 0), N >> 3 in bits 17-22, M >> 4 in bits 24-28.
-__host__ __device__ constexpr uint32_t idesc_f16(int m, int n, bool a_mn_major, bool neg_a = false)
+// Instruction descriptor, kind::f16: f32 accumulator (bits 4-5 = 1), A and
+// B of one type (bits 7-9 and 10-12: 0 f16, 1 bf16), negate A (bit 13), A
+// MN-major (bit 15), B K-major (bit 16 = 0), N >> 3 in bits 17-22, M >> 4 in
+// bits 24-28.
+__host__ __device__ constexpr uint32_t idesc_f16(int m, int n, bool a_mn_major, bool neg_a = false,
+                                                 uint32_t fmt = 0)
 {
-    return (1u << 4) | ((neg_a ? 1u : 0u) << 13) | ((a_mn_major ? 1u : 0u) << 15) | ((uint32_t)(n >> 3) << 17) |
-           ((uint32_t)(m >> 4) << 24);
+    return (1u << 4) | (fmt << 7) | (fmt << 10) | ((neg_a ? 1u : 0u) << 13) | ((a_mn_major ? 1u : 0u) << 15) |
+           ((uint32_t)(n >> 3) << 17) | ((uint32_t)(m >> 4) << 24);
 }
 
 }  // namespace tc

@@ -70,14 +70,14 @@ class Dedisperser:
     the minimum like the reference does.  ``series`` materialises the
     dedispersed series (needed by get_output); ``osm`` selects classical
     overlap-save.  ``precision`` "fp32" (default) runs the inverse transforms
-    on the CUDA cores in FP32; "fp16" runs them on the tensor cores with f16
-    operands and f32 accumulation (FFT size 4096 only).
+    on the CUDA cores in FP32; "fp16" / "bf16" run them on the tensor cores
+    with f16 / bf16 operands and f32 accumulation (FFT size 4096 only).
     """
 
     def __init__(self, bw, dm, f0, fftpoint: int = 0, count: int = 1, input_size: int = 0,
                  osm: bool = False, series: bool = True, precision: str = "fp32"):
-        if precision not in ("fp32", "fp16"):
-            raise ValueError("precision must be 'fp32' or 'fp16'")
+        if precision not in ("fp32", "fp16", "bf16"):
+            raise ValueError("precision must be 'fp32', 'fp16' or 'bf16'")
         dm = _f32_array(dm)
         n = dm.size
         bw = _f32_array(bw, n)
@@ -86,7 +86,8 @@ class Dedisperser:
             raise ValueError("bw, dm, f0 must be scalars or arrays of one length")
         self._params = (bw, dm, f0)
         flags = ((_abi.FLAG_OSM if osm else 0) | (0 if series else _abi.FLAG_NO_SERIES)
-                 | (_abi.FLAG_TENSOR_F16 if precision == "fp16" else 0))
+                 | (_abi.FLAG_TENSOR_F16 if precision == "fp16" else 0)
+                 | (_abi.FLAG_TENSOR_BF16 if precision == "bf16" else 0))
         h = ctypes.c_void_p()
         check(lib().msosm_dedisp_create(bw.ctypes.data, dm.ctypes.data, f0.ctypes.data, n,
                                         int(fftpoint), int(count), int(input_size), flags,

@@ -55,6 +55,9 @@ def test_tensor_path_rejects_other_fft_sizes():
                                         _abi.FLAG_TENSOR_F16, ctypes.byref(h))
     assert st == _abi.ERR_UNSUPPORTED and not h.value
     assert b"4096" in _abi.lib().msosm_last_error()
+    st = _abi.lib().msosm_dedisp_create(bw.ctypes.data, dm.ctypes.data, f0.ctypes.data, 1, 4096, 4, 0,
+                                        _abi.FLAG_TENSOR_F16 | _abi.FLAG_TENSOR_BF16, ctypes.byref(h))
+    assert st == _abi.ERR_BAD_ARG and not h.value
 
 
 def test_tensor_layout_tables():

@@ -5,8 +5,11 @@ against the FP64 oracle and against the FP32 CUDA-core path.
 Error budget (stated, not tuned): f16 operands carry a relative rounding of
 2^-11 at four places (gathered products, DFT constants, twiddled
 intermediates, second DFT constants), which gives a series error near 5e-4
-relative RMS; the tests bound it at 1.5e-3.  Folded profiles average many
-samples per bin and are bound at 1e-4."""
+relative RMS; the tests bound it at 1.5e-3.  bf16 (2^-8 rounding) gives about
+eight times that; bound 1e-2.  Folded profiles average many samples per bin
+and are bound at 1e-4 (f16); with bf16 the rounded DFT constants leave a
+systematic gain error that averaging does not remove (measured 1.5e-3 here),
+bound 5e-3."""
 import numpy as np
 import pytest
 
@@ -19,6 +22,7 @@ pytestmark = pytest.mark.gpu
 BW, F0 = 16e6, 1242e6
 SERIES_TOL = 1.5e-3
 FOLD_TOL = 1e-4
+TOL = {"fp16": (SERIES_TOL, FOLD_TOL), "bf16": (1e-2, 5e-3)}
 
 
 def rel_rms(a, b):
@@ -56,8 +60,8 @@ def u16(n, seed, scale=1000.0):
     return np.clip(np.rint(rng.standard_normal((n, 2)) * scale) + 32768, 1, 65535).astype(np.uint16)
 
 
-def run_pair(dms, count, calls, seed=0, series=True, x=None):
-    d = Dedisperser(BW, dms, F0, 4096, count, precision="fp16", series=series)
+def run_pair(dms, count, calls, seed=0, series=True, x=None, precision="fp16"):
+    d = Dedisperser(BW, dms, F0, 4096, count, precision=precision, series=series)
     o = O.Dedisp(BW, dms, F0, 4096, count)
     if x is None:
         x = u16(d.block_samples * calls, seed)
@@ -70,16 +74,17 @@ def run_pair(dms, count, calls, seed=0, series=True, x=None):
     return np.concatenate(ours, 1), np.concatenate(ref, 1), d, x
 
 
+@pytest.mark.parametrize("precision", ["fp16", "bf16"])
 @pytest.mark.parametrize("count,calls", [(6, 3), (5, 4), (1, 5)])
-def test_series_matches_oracle(count, calls):
+def test_series_matches_oracle(count, calls, precision):
     # DM 0 (no delay), short delays (warm ring after a few blocks) and long
     # ones (blocks before the stream start read as zero); odd counts leave
     # the last block of a call unpaired
     dms = [0.0, 2.0, 5.0, 40.0, 100.0]
-    ours, ref, _, _ = run_pair(dms, count, calls, seed=count)
+    ours, ref, _, _ = run_pair(dms, count, calls, seed=count, precision=precision)
     for i in range(len(dms)):
         e = rel_rms(ours[i], ref[i])
-        assert e < SERIES_TOL, (dms[i], e)
+        assert e < TOL[precision][0], (dms[i], e)
 
 
 def test_series_matches_fp32_path():
@@ -126,9 +131,10 @@ def test_full_scale_tone_stays_finite_and_accurate():
         assert rel_rms(ours[i], ref[i]) < SERIES_TOL
 
 
-def test_fold_matches_oracle():
+@pytest.mark.parametrize("precision", ["fp16", "bf16"])
+def test_fold_matches_oracle(precision):
     dms, count, calls, period, tb = [0.0, 20.0, 73.2], 8, 6, 0.0011, 256
-    d = Dedisperser(BW, dms, F0, 4096, count, series=False, precision="fp16")
+    d = Dedisperser(BW, dms, F0, 4096, count, series=False, precision=precision)
     nd = 4096
     d.fold_init(period, BW, time_bin=tb, discard_Nd=nd)
     o = O.Dedisp(BW, dms, F0, 4096, count)
@@ -147,4 +153,4 @@ def test_fold_matches_oracle():
         for c in range(calls):
             f.fold_data(np.abs(ser[i, c * d.block_samples:(c + 1) * d.block_samples]) ** 2)
         e = rel_rms(prof[i], f.fold_data_bins())
-        assert e < FOLD_TOL, (dms[i], e)
+        assert e < TOL[precision][1], (dms[i], e)
