@@ -123,9 +123,9 @@ typedef struct msosm_dedisp msosm_dedisp;
 /* flags for msosm_dedisp_create */
 #define MSOSM_FLAG_OSM 0x1u      /* classical overlap-save (OSM_GPU_*) instead of MS-OSM */
 #define MSOSM_FLAG_NO_SERIES 0x2u /* do not materialise the dedispersed series (fold only) */
-/* Inverse transforms on the tensor cores: f16 operands with a per-block
- * power-of-two scale, f32 accumulation.  No counterpart in the reference
- * (its inverse transform is the FP32 cuFFT).  FFT size 4096 only (other
+/* Inverse transforms on the tensor cores: f16 operands with a power-of-two
+ * scale per work item, f32 accumulation.  No counterpart in the reference
+ * (its inverse transform is the FP32 cuFFT).  FFT sizes 4096 and 8192 (other
  * sizes return MSOSM_ERR_UNSUPPORTED).  Relative RMS error of the series
  * against FP64: about 5e-4; folded profiles much lower. */
 #define MSOSM_FLAG_TENSOR_F16 0x4u
@@ -333,13 +333,15 @@ MSOSM_API msosm_status msosm_dada_read(msosm_dada *d, unsigned long n, msosm_uin
  * Diagnostics (no counterpart in the reference)
  * ====================================================================== */
 
-/* Runs one of the two tensor-core GEMMs of MSOSM_FLAG_TENSOR_F16 on given
- * data, with the kernel's own shared-memory layouts, constant operand and
- * tensor-memory read-back: d = a * B_step, where a is a 128 x 128 matrix of
- * f16 bit patterns (row-major, host memory) and B_step the real form of the
- * 64-point inverse DFT (step 1: 128 x 128, outputs [Re | Im] of all 64
- * frequencies; step 2: 128 x 64, outputs [Re | Im] of frequencies 32..63).
- * d: host, 128 x (step 1 ? 128 : 64) floats, row-major.  Needs a GPU. */
+/* Runs one of the tensor-core GEMMs of MSOSM_FLAG_TENSOR_F16 on given data,
+ * with the kernel's own shared-memory layouts, constant operand and
+ * tensor-memory read-back: d = a * B_step, a a 128 x K matrix of f16 bit
+ * patterns (row-major, host memory), B_step the real form of an inverse DFT
+ * with rows [Re | Im] of the input index and columns [Re | Im] of the output
+ * frequency.  Step 1: the 64-point DFT of FFT 4096 (K 128, 128 columns);
+ * step 2: the 64-point DFT restricted to frequencies 32..63 (K 128, 64
+ * columns); step 3: the 128-point DFT of FFT 8192 (K 256, 256 columns).
+ * d: host, 128 x columns floats, row-major.  Needs a GPU. */
 MSOSM_API msosm_status msosm_tc_gemm_check(int step, const uint16_t *a, float *d);
 
 #ifdef __cplusplus

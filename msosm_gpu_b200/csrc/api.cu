@@ -229,6 +229,11 @@ msosm_status design_filters(int log2n, const std::vector<ChirpParams> &cp, float
     return MSOSM_OK;
 }
 
+// Profiles of up to this many bins live in shared memory inside the fused
+// kernel (beyond it, in the global partial rows): the 8192-point tensor-core
+// kernel leaves room for 2048.
+int smem_bins_limit(const msosm_dedisp *d) { return d->tc && d->log2n == 13 ? 2048 : kMaxSmemBins; }
+
 // Persistent grid of the dedispersion kernel: work items (block range,
 // trial), about eight per resident CTA, spread evenly over the waves.
 cudaError_t plan_grid(msosm_dedisp *d)
@@ -239,9 +244,9 @@ cudaError_t plan_grid(msosm_dedisp *d)
         e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     if (e != cudaSuccess)
         return e;
-    const int threads = d->tc ? tc::kThreads : (int)(d->N / 16);
-    const size_t extra = d->fold ? fold_smem_bytes(d->nbins, d->win_cap, d->nbins <= kMaxSmemBins, threads) : 0;
-    int per_sm = d->tc ? tc_blocks_per_sm(d->tc_bf16, d->series, d->fold, extra)
+    const int threads = d->tc ? tc_threads(d->log2n) : (int)(d->N / 16);
+    const size_t extra = d->fold ? fold_smem_bytes(d->nbins, d->win_cap, d->nbins <= smem_bins_limit(d), threads) : 0;
+    int per_sm = d->tc ? tc_blocks_per_sm(d->log2n, d->tc_bf16, d->series, d->fold, extra)
                        : dedisp_blocks_per_sm(d->log2n, d->pingpong, d->series, d->fold, extra);
     if (per_sm < 1)
         per_sm = 1;
@@ -527,7 +532,7 @@ msosm_status msosm_dedisp_create(const float *bw, const float *dm, const float *
     }
     if (d->tc && !tc_supported(log2n)) {
         release(d);
-        return fail(MSOSM_ERR_UNSUPPORTED, "the tensor-core path needs FFT size %d (got %lu)", tc::kN, 2 * M);
+        return fail(MSOSM_ERR_UNSUPPORTED, "the tensor-core path needs FFT size 4096 or 8192 (got %lu)", 2 * M);
     }
     if (input_size != 0)
         count = (int)(input_size / M);
@@ -617,7 +622,7 @@ msosm_status msosm_dedisp_create(const float *bw, const float *dm, const float *
         for (int t = 0; t < numDMs; ++t)
             for (unsigned long p = 0; p < N; ++p) {
                 const unsigned long b = d->large ? (p / N2) + N1 * (p % N2) : p;
-                const unsigned long q = d->tc ? (unsigned long)tc::tc_pos((int)p) : p;
+                const unsigned long q = d->tc ? (unsigned long)tc::tc_pos((int)p, log2n) : p;
                 dl[(size_t)t * N + q] = (uint16_t)d->delays[(size_t)t * N + b];
             }
         CKD(cudaMemcpy(d->delays_d, dl.data(), sizeof(uint16_t) * dl.size(), cudaMemcpyHostToDevice));
@@ -642,7 +647,7 @@ msosm_status msosm_dedisp_create(const float *bw, const float *dm, const float *
         if (d->tc) {
             float2 *tmp = nullptr;
             CKD(cudaMalloc((void **)&tmp, sizeof(float2) * (size_t)numDMs * N));
-            cudaError_t e = launch_tc_permute_rows(d->H, tmp, numDMs, d->stream);
+            cudaError_t e = launch_tc_permute_rows(d->H, tmp, numDMs, log2n, d->stream);
             if (e == cudaSuccess)
                 e = cudaMemcpyAsync(d->H, tmp, sizeof(float2) * (size_t)numDMs * N, cudaMemcpyDeviceToDevice,
                                     d->stream);
@@ -751,7 +756,7 @@ msosm_status msosm_dedisp_get_dedisp_params(const msosm_dedisp *d, int i, msosm_
     const unsigned long N1 = 1ul << d->log2n1, N2 = 1ul << d->log2n2;
     for (unsigned long b = 0; b < d->N; ++b) {
         // four-step layout: bin b = k1 + N1*k2 sits at k1*N2 + k2
-        const unsigned long p = d->large ? (b % N1) * N2 + b / N1 : (d->tc ? (unsigned long)tc::tc_pos((int)b) : b);
+        const unsigned long p = d->large ? (b % N1) * N2 + b / N1 : (d->tc ? (unsigned long)tc::tc_pos((int)b, d->log2n) : b);
         H[b].x = tmp[p].x * up;
         H[b].y = tmp[p].y * up;
     }
@@ -808,7 +813,7 @@ static msosm_status fold_prepare(msosm_dedisp *d, int sb, FoldArgs &fa)
     fa.detect = d->detect;
     fa.part_main = d->part_main;
     fa.part_pend = d->part_pend;
-    fa.smem_prof = d->nbins <= kMaxSmemBins ? 1 : 0;
+    fa.smem_prof = d->nbins <= smem_bins_limit(d) ? 1 : 0;
     fa.span_cap = d->win_cap;
     fa.inv_bpt = 1.0f / (float)d->bpt;
     fa.g_shift = fold_g_shift(d->bpt, d->large ? 256 : (int)(d->N / 16));
@@ -988,7 +993,7 @@ static msosm_status filter_block(msosm_dedisp *d, const void *input, InputKind k
     if (ev)
         CK(cudaEventRecord(ev->e[2], d->stream));
     if (d->tc)
-        CK(launch_tc_dedisp(d->tc_bf16, d->series, d->fold, da, d->grid, d->stream));
+        CK(launch_tc_dedisp(d->log2n, d->tc_bf16, d->series, d->fold, da, d->grid, d->stream));
     else
         CK(launch_dedisp(d->log2n, d->pingpong, d->series, d->fold, da, d->grid, d->stream));
     d->launches += 1;
@@ -1525,11 +1530,12 @@ msosm_status msosm_fold_planner_chunk(msosm_fold_planner *p, unsigned long size,
 
 msosm_status msosm_tc_gemm_check(int step, const uint16_t *a, float *d)
 {
-    if ((step != 1 && step != 2) || !a || !d)
-        return fail(MSOSM_ERR_BAD_ARG, "step must be 1 or 2; a and d non-null");
+    if (step < 1 || step > 3 || !a || !d)
+        return fail(MSOSM_ERR_BAD_ARG, "step must be 1, 2 or 3; a and d non-null");
     if (msosm_device_count() == 0)
         return fail(MSOSM_ERR_NO_DEVICE, "no CUDA device");
-    const size_t na = 128 * 128, nd = (size_t)128 * (step == 1 ? 128 : 64);
+    const size_t na = (size_t)128 * (step == 3 ? 256 : 128);
+    const size_t nd = (size_t)128 * (step == 3 ? 256 : (step == 1 ? 128 : 64));
     uint16_t *ad = nullptr;
     float *dd = nullptr;
     int *st = nullptr;

@@ -115,19 +115,22 @@ int fold_series_block();
 cudaError_t launch_fold_series(const float *I, long long n, int R, const FoldArgs &f, int grid, int trials,
                                cudaStream_t st);
 
-// ---- tensor-core (tcgen05) dedispersion, 4096-point transforms (tc_dedisp.cu)
+// ---- tensor-core (tcgen05) dedispersion, 4096- and 8192-point transforms (tc_dedisp.cu)
 bool tc_supported(int log2n);
-// dynamic shared memory of the tensor-core kernel with `extra` fold bytes
-size_t tc_smem_bytes(size_t extra);
-int tc_blocks_per_sm(bool bf16, bool series, bool fold, size_t extra_smem);
+// threads per CTA of the tensor-core kernel (its fold group size)
+int tc_threads(int log2n);
+int tc_blocks_per_sm(int log2n, bool bf16, bool series, bool fold, size_t extra_smem);
 // a.H and a.delays in tensor-core order (tc_layout.hpp), ring written with
-// FwdArgs::tc_order; a.R counts ranges of block pairs
-// bf16: bf16 operands (else f16)
-cudaError_t launch_tc_dedisp(bool bf16, bool series, bool fold, const DedispArgs &a, int grid, cudaStream_t st);
-// rows of n bins (n = 4096) from natural into tensor-core order, in place via scratch
-cudaError_t launch_tc_permute_rows(const float2 *in, float2 *out, int rows, cudaStream_t st);
-// one GEMM of the kernel on given data: a = 128 x 128 f16 bit patterns
-// (row-major, M x K), d = 128 x (step 1 ? 128 : 64) f32 (row-major)
+// FwdArgs::tc_order; a.R counts ranges of block pairs; bf16: bf16 operands
+// (else f16)
+cudaError_t launch_tc_dedisp(int log2n, bool bf16, bool series, bool fold, const DedispArgs &a, int grid,
+                             cudaStream_t st);
+// rows of 2^log2n bins from natural into tensor-core order (out of place)
+cudaError_t launch_tc_permute_rows(const float2 *in, float2 *out, int rows, int log2n, cudaStream_t st);
+// one GEMM of the kernel on given data: a = 128 x K f16 bit patterns
+// (row-major), d = 128 x columns f32 (row-major); steps 1, 2: the
+// 4096-point GEMMs (K 128; 128 and 64 columns), 3: the 8192-point GEMM 1
+// (K 256, 256 columns)
 cudaError_t launch_tc_probe(int step, const uint16_t *a, float *d, int *status, cudaStream_t st);
 
 // ---- FFT sizes above one thread block (largefft.cu) -----------------------

@@ -173,15 +173,6 @@ __device__ __forceinline__ void st_shared_v4(unsigned char *p, uint32_t a, uint3
     *reinterpret_cast<uint4 *>(p) = make_uint4(a, b, c, d);
 }
 
-// 2^e with 2^e * mx < 2^8, and its inverse (exponent arithmetic, exact)
-__device__ __forceinline__ void pow2_scale(float mx, float &s, float &inv)
-{
-    int e = (__float_as_int(mx) >> 23) & 0xFF;
-    e = min(max(e, 8), 254);
-    s = __int_as_float((261 - e) << 23);
-    inv = __int_as_float((e - 7) << 23);
-}
-
 __device__ __forceinline__ float warp_max(float v)
 {
 #pragma unroll
@@ -190,79 +181,106 @@ __device__ __forceinline__ float warp_max(float v)
     return v;
 }
 
-// The constant operands: [C | S] of the 64-point inverse DFT, K-major.
-//   GEMM 1, B1[n][k2], k2 < 64: n < 64 -> cos(2 pi k2 n / 64),
-//     n >= 64 -> sin(2 pi k2 (n - 64) / 64)            (output frequency m2)
+// The constant operands, K-major: [C | S] of the N2-point inverse DFT for
+// GEMM 1 and of the 64-point one (outputs m1 = 32..63) for GEMM 2.
+//   GEMM 1, B1[n][k2], k2 < N2: n < N2 -> cos(2 pi k2 n / N2),
+//     n >= N2 -> sin(2 pi k2 (n - N2) / N2)           (output frequency m2)
 //   GEMM 2, B2[n][k1], k1 < 64: n < 32 -> cos(2 pi k1 (32 + n) / 64),
 //     n >= 32 -> sin(2 pi k1 n / 64)                   (output m1 = 32..63)
-template <class E>
+template <class E, int LOG2N>
 __device__ void fill_constants(unsigned char *sm, int tid)
 {
-    for (int e = tid; e < 128 * 64; e += kThreads) {
-        const int n = e >> 6, k = e & 63;
+    using S = TcShape<LOG2N>;
+    constexpr int N2 = S::N2;
+    for (int e = tid; e < 2 * N2 * N2; e += (int)blockDim.x) {
+        const int n = e / N2, k = e % N2;
         float s, c;
-        sincospif((float)((k * (n & 63)) & 63) * (1.0f / 32.0f), &s, &c);
-        *reinterpret_cast<typename E::h1 *>(sm + kSmemB1 + k_off(n, k)) = E::one(n < 64 ? c : s);
+        sincospif((float)((k * (n & (N2 - 1))) & (N2 - 1)) * (2.0f / N2), &s, &c);
+        *reinterpret_cast<typename E::h1 *>(sm + S::SMEM_B1 + k_off(n, k, (int)S::SBO_B1)) = E::one(n < N2 ? c : s);
     }
-    for (int e = tid; e < 64 * 64; e += kThreads) {
+    for (int e = tid; e < 64 * 64; e += (int)blockDim.x) {
         const int n = e >> 6, k = e & 63;
         float s, c;
         sincospif((float)((k * (32 + (n & 31))) & 63) * (1.0f / 32.0f), &s, &c);
-        *reinterpret_cast<typename E::h1 *>(sm + kSmemB2 + k_off(n, k)) = E::one(n < 32 ? c : s);
+        *reinterpret_cast<typename E::h1 *>(sm + S::SMEM_B2 + k_off(n, k)) = E::one(n < 32 ? c : s);
     }
 }
 
 // mbarriers (GEMM 1, GEMM 2) + tensor memory; every thread returns the TMEM base
+template <int LOG2N>
 __device__ uint32_t tc_setup(unsigned char *sm, uint32_t s0, int tid, int warp)
 {
+    using S = TcShape<LOG2N>;
     if (tid == 0) {
-        mbar_init(s0 + kSmemCtl, 1);
-        mbar_init(s0 + kSmemCtl + 8, 1);
+        mbar_init(s0 + S::SMEM_CTL, 1);
+        mbar_init(s0 + S::SMEM_CTL + 8, 1);
         fence_mbar_init();
     }
     if (warp == 0) {
-        tmem_alloc(s0 + kSmemCtl + 16, kTmemCols);
+        tmem_alloc(s0 + S::SMEM_CTL + 16, S::TMEM_COLS);
         tmem_relinquish();
     }
     fence_proxy_async();  // shared-memory operands written so far -> tensor core
     tc_fence_before();
     __syncthreads();
     tc_fence_after();
-    return *reinterpret_cast<volatile uint32_t *>(sm + kSmemCtl + 16);
+    return *reinterpret_cast<volatile uint32_t *>(sm + S::SMEM_CTL + 16);
 }
 
+template <int LOG2N>
 __device__ __forceinline__ void tc_teardown(uint32_t tmem, int warp)
 {
     tc_fence_before();
     __syncthreads();
     if (warp == 0) {
         tc_fence_after();
-        tmem_dealloc(tmem, kTmemCols);
+        tmem_dealloc(tmem, TcShape<LOG2N>::TMEM_COLS);
     }
 }
 
-// One complex GEMM: D (n2 = 2 * half columns: [Re | Im]) = data (128 x [Re |
-// Im] K = 128, MN-major at a) x the DFT whose [C | S] (K = 64, n2 columns)
-// is at b; then the commit to the mbarrier.  Three passes of four K = 16
-// steps: Re x [C | S], then -Im x S into the Re half, Im x C into the Im half.
+// One complex GEMM: D (2 half columns: [Re | Im]) = data (128 rows x [Re |
+// Im], K = 2 x 16 ksteps, MN-major at a) x the DFT whose [C | S] (K = 16
+// ksteps, 2 half columns, N-group stride sbo) is at b.  Three passes of
+// ksteps K = 16 steps: Re x [C | S], then -Im x S into the Re half, Im x C
+// into the Im half.
 template <class E>
-__device__ __forceinline__ void issue_cgemm(uint32_t tmem_d, uint32_t a, uint32_t b, int half, uint32_t bar)
+__device__ __forceinline__ void issue_cgemm(uint32_t tmem_d, uint32_t a, uint32_t b, int half, int ksteps,
+                                            uint32_t sbo)
 {
     const uint32_t id_full = idesc_f16(128, 2 * half, true, false, E::fmt);
     const uint32_t id_neg = idesc_f16(128, half, true, true, E::fmt);
     const uint32_t id_half = idesc_f16(128, half, true, false, E::fmt);
-#pragma unroll
-    for (int s = 0; s < 4; ++s)
-        mma_f16(tmem_d, smem_desc(a + s * kDescStepA, 2048, 128), smem_desc(b + s * kDescStepB, 128, 1024),
-                id_full, s > 0 ? 1u : 0u);
-#pragma unroll
-    for (int s = 0; s < 4; ++s)
-        mma_f16(tmem_d, smem_desc(a + (4 + s) * kDescStepA, 2048, 128),
-                smem_desc(b + b_col(half) + s * kDescStepB, 128, 1024), id_neg, 1u);
-#pragma unroll
-    for (int s = 0; s < 4; ++s)
-        mma_f16(tmem_d + half, smem_desc(a + (4 + s) * kDescStepA, 2048, 128),
-                smem_desc(b + s * kDescStepB, 128, 1024), id_half, 1u);
+    for (int s = 0; s < ksteps; ++s)
+        mma_f16(tmem_d, smem_desc(a + s * kDescStepA, 2048, 128), smem_desc(b + s * kDescStepB, 128, sbo), id_full,
+                s > 0 ? 1u : 0u);
+    const uint32_t bs = b + (uint32_t)(half >> 3) * sbo;
+    for (int s = 0; s < ksteps; ++s)
+        mma_f16(tmem_d, smem_desc(a + (ksteps + s) * kDescStepA, 2048, 128),
+                smem_desc(bs + s * kDescStepB, 128, sbo), id_neg, 1u);
+    for (int s = 0; s < ksteps; ++s)
+        mma_f16(tmem_d + half, smem_desc(a + (ksteps + s) * kDescStepA, 2048, 128),
+                smem_desc(b + s * kDescStepB, 128, sbo), id_half, 1u);
+}
+
+// GEMM 1 of a pair (operand buffer at a), committed to bar
+template <class E, int LOG2N>
+__device__ __forceinline__ void issue_gemm1(uint32_t tmem, uint32_t s0, uint32_t a, uint32_t bar)
+{
+    using S = TcShape<LOG2N>;
+    issue_cgemm<E>(tmem, a, s0 + S::SMEM_B1, S::N2, S::N2 / 16, S::SBO_B1);
+    mma_commit(bar);
+}
+
+// GEMM 2 of a pair: one GEMM for both blocks at N = 4096 (rows 64 b + m2),
+// one per block at N = 8192 (block b's operand 32 KB on, its result 64
+// columns on), committed to bar
+template <class E, int LOG2N>
+__device__ __forceinline__ void issue_gemm2(uint32_t tmem, uint32_t s0, uint32_t a, uint32_t bar)
+{
+    using S = TcShape<LOG2N>;
+    issue_cgemm<E>(tmem + S::D2_COL, a, s0 + S::SMEM_B2, 32, 4, 1024);
+    if constexpr (S::N2 == 128)
+        issue_cgemm<E>(tmem + S::D2_COL + 64, a + 32768, s0 + S::SMEM_B2, 32, 4, 1024);
     mma_commit(bar);
 }
 
@@ -281,34 +299,52 @@ __device__ __forceinline__ bool wait_gemm(int tid, uint32_t bar, uint32_t &parit
     return !failed;
 }
 
-template <class E, bool SERIES, bool FOLD>
-__global__ void __launch_bounds__(kThreads, 2) tc_dedisp_kernel(DedispArgs a)
+// 2^e with 2^e * mx < 2^X, and its inverse (exponent arithmetic, exact)
+template <int X>
+__device__ __forceinline__ void pow2_scale_to(float mx, float &s, float &inv)
 {
+    int e = (__float_as_int(mx) >> 23) & 0xFF;
+    e = min(max(e, X), 254);
+    s = __int_as_float((X + 253 - e) << 23);
+    inv = __int_as_float((e - X + 1) << 23);
+}
+
+template <int LOG2N, class E, bool SERIES, bool FOLD>
+__global__ void __launch_bounds__(TcShape<LOG2N>::THREADS, TcShape<LOG2N>::CTAS_PER_SM)
+    tc_dedisp_kernel(DedispArgs a)
+{
+    using S = TcShape<LOG2N>;
+    constexpr int N = S::N, M = S::M, N2 = S::N2, W = S::WARPS, T = S::THREADS;
     extern __shared__ __align__(1024) unsigned char sm[];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t s0 = smem_addr(sm);
-    const uint32_t barA = s0 + kSmemCtl, barB = s0 + kSmemCtl + 8;
+    const uint32_t barA = s0 + S::SMEM_CTL, barB = s0 + S::SMEM_CTL + 8;
     FoldSmem fw;
     if constexpr (FOLD)
-        fold_smem_layout(fw, sm + kSmemFold, a.fold);
-    fill_constants<E>(sm, tid);
-    const uint32_t tmem = tc_setup(sm, s0, tid, warp);
+        fold_smem_layout(fw, sm + S::SMEM_FOLD, a.fold);
+    fill_constants<E, LOG2N>(sm, tid);
+    const uint32_t tmem = tc_setup<LOG2N>(sm, s0, tid, warp);
     // epilogue view: warp w reads TMEM lanes 32 (w % 4) .. + 31 (its GEMM
-    // rows) and half h = w / 4 of the columns
+    // rows) and column group g = w / 4
     const uint32_t lane_base = (uint32_t)(32 * (warp & 3)) << 16;
-    const uint32_t tD1 = tmem + lane_base, tD2 = tmem + lane_base + 128;
-    const int h = warp >> 2;
+    const uint32_t tD1 = tmem + lane_base, tD2 = tmem + lane_base + S::D2_COL;
+    const int g = warp >> 2;
     const int row = 32 * (warp & 3) + lane;
-    const int rb = row >> 6, ri = row & 63;  // block of the pair; k1 (GEMM 1) / m2 (GEMM 2)
-    // this thread's twiddles e^{+2 pi i ri m2 / 4096}, m2 = 32 h + i, as f16
+    const int rb = row >> 6, ri = row & 63;  // GEMM 1 row: block of the pair, k1
+    // GEMM 2 rows: N = 4096 -> (block rb, m2 = ri); N = 8192 -> (block g % 2, m2 = row)
+    const int ob = N2 == 64 ? rb : (g & 1);
+    const int om2 = N2 == 64 ? ri : row;
+    const int oh = N2 == 64 ? g : (g >> 1);  // output columns c = 16 oh .. 16 oh + 15
+    const uint32_t tD2b = tD2 + (N2 == 64 ? 0u : 64u * (uint32_t)ob);
+    // this thread's twiddles e^{+2 pi i ri m2 / N}, m2 = 32 g + i, as 16-bit
     // pairs (m2, m2 + 1) matching the operand packing
     typename E::h2 twr[16], twi[16];
 #pragma unroll
     for (int i = 0; i < 16; ++i) {
         float s0f, c0f, s1f, c1f;
-        const int m2 = 32 * h + 2 * i;
-        sincospif((float)((ri * m2) & 4095) * (1.0f / 2048.0f), &s0f, &c0f);
-        sincospif((float)((ri * (m2 + 1)) & 4095) * (1.0f / 2048.0f), &s1f, &c1f);
+        const int m2 = 32 * g + 2 * i;
+        sincospif((float)((ri * m2) & (N - 1)) * (2.0f / N), &s0f, &c0f);
+        sincospif((float)((ri * (m2 + 1)) & (N - 1)) * (2.0f / N), &s1f, &c1f);
         twr[i] = E::pack(c0f, c1f);
         twi[i] = E::pack(s0f, s1f);
     }
@@ -331,12 +367,12 @@ __global__ void __launch_bounds__(kThreads, 2) tc_dedisp_kernel(DedispArgs a)
         float4 hreg[8];
         uint32_t dd[8];
         {
-            const float4 *__restrict__ H4 = reinterpret_cast<const float4 *>(a.H + (size_t)dm * kN);
-            const uint32_t *__restrict__ dl2 = reinterpret_cast<const uint32_t *>(a.delays + (size_t)dm * kN);
+            const float4 *__restrict__ H4 = reinterpret_cast<const float4 *>(a.H + (size_t)dm * N);
+            const uint32_t *__restrict__ dl2 = reinterpret_cast<const uint32_t *>(a.delays + (size_t)dm * N);
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
-                dd[j] = __ldg(dl2 + (j * 8 + warp) * 32 + lane);
-                hreg[j] = __ldg(H4 + (j * 8 + warp) * 32 + lane);
+                dd[j] = __ldg(dl2 + (j * W + warp) * 32 + lane);
+                hreg[j] = __ldg(H4 + (j * W + warp) * 32 + lane);
             }
         }
         // power-of-two scale of the work item: |Z| <= 2 max|X| max|H| over
@@ -345,18 +381,18 @@ __global__ void __launch_bounds__(kThreads, 2) tc_dedisp_kernel(DedispArgs a)
         {
             float wm = 0.f;
             const long long r_hi = a.k0 + ke - 1;
-            for (long long r = a.k0 + kb - __ldg(a.delay_max + dm) + tid; r <= r_hi; r += kThreads)
+            for (long long r = a.k0 + kb - __ldg(a.delay_max + dm) + tid; r <= r_hi; r += T)
                 if (r >= 0)
                     wm = fmaxf(wm, a.row_max[r & smask]);
             wm = warp_max(wm);
-            float *wmax = reinterpret_cast<float *>(sm + kSmemCtl + 32);
+            float *wmax = reinterpret_cast<float *>(sm + S::SMEM_CTL + 32);
             if (lane == 0)
                 wmax[warp] = wm;
             __syncthreads();
 #pragma unroll
-            for (int i = 0; i < kThreads / 32; ++i)
+            for (int i = 0; i < W; ++i)
                 wm = fmaxf(wm, wmax[i]);
-            pow2_scale(2.0f * wm * __ldg(a.h_max + dm), sc, isc);
+            pow2_scale_to<S::SCALE_EXP>(2.0f * wm * __ldg(a.h_max + dm), sc, isc);
 #pragma unroll
             for (int j = 0; j < 8; ++j)
                 hreg[j] = make_float4(hreg[j].x * sc, hreg[j].y * sc, hreg[j].z * sc, hreg[j].w * sc);
@@ -370,14 +406,13 @@ __global__ void __launch_bounds__(kThreads, 2) tc_dedisp_kernel(DedispArgs a)
                 fw.prof_main = a.fold.part_main + (size_t)w * a.fold.nbins;
                 fw.prof_pend = a.fold.part_pend + (size_t)w * a.fold.nbins;
             }
-            sp = span_lower_bound(a.fold.span_b, a.fold.nspans, (long long)kb * kM);
+            sp = span_lower_bound(a.fold.span_b, a.fold.nspans, (long long)kb * M);
             span_refill(a.fold, fw, sp, sbase, scnt);
         }
 
         // Gather pair i of the item (blocks k, k + 1) into operand buffer
         // `op`: Z = X[kg + b - delay][bin] * H[bin] * sc, element (row 64 b
-        // + k1, k = k2) of the MN-major operand, Im parts 8 core-matrix
-        // columns on.
+        // + k1, k = k2) of the MN-major operand, Im parts N2 K-columns on.
         auto gather = [&](int i, unsigned char *op) {
             const int k = kb + 2 * i;
             const bool two = k + 1 < ke;
@@ -387,20 +422,20 @@ __global__ void __launch_bounds__(kThreads, 2) tc_dedisp_kernel(DedispArgs a)
                 // every delayed block exists: no zero fill
 #pragma unroll
                 for (int j = 0; j < 8; ++j) {
-                    const int q = (j * 8 + warp) * 32 + lane;  // float4 (bin pair) index in a row
+                    const int q = (j * W + warp) * 32 + lane;  // float4 (bin pair) index in a row
                     const float4 hv = hreg[j];
                     const int d0 = (int)(dd[j] & 0xFFFFu), d1 = (int)(dd[j] >> 16);
                     float4 x[2];
                     if (d0 == d1) {
                         const int r = (slot0 - d0) & smask;
-                        x[0] = ring4[(size_t)r * (kN / 2) + q];
-                        x[1] = ring4[(size_t)((r + 1) & smask) * (kN / 2) + q];
+                        x[0] = ring4[(size_t)r * (N / 2) + q];
+                        x[1] = ring4[(size_t)((r + 1) & smask) * (N / 2) + q];
                     } else {
                         const int r0 = (slot0 - d0) & smask, r1 = (slot0 - d1) & smask;
 #pragma unroll
                         for (int b = 0; b < 2; ++b) {
-                            const float2 t0 = ring2[(size_t)((r0 + b) & smask) * kN + 2 * q];
-                            const float2 t1 = ring2[(size_t)((r1 + b) & smask) * kN + 2 * q + 1];
+                            const float2 t0 = ring2[(size_t)((r0 + b) & smask) * N + 2 * q];
+                            const float2 t1 = ring2[(size_t)((r1 + b) & smask) * N + 2 * q + 1];
                             x[b] = make_float4(t0.x, t0.y, t1.x, t1.y);
                         }
                     }
@@ -410,13 +445,13 @@ __global__ void __launch_bounds__(kThreads, 2) tc_dedisp_kernel(DedispArgs a)
                         const float zr1 = x[b].z * hv.z - x[b].w * hv.w, zi1 = x[b].z * hv.w + x[b].w * hv.z;
                         const int off = (b * 8 + j) * 128 + warp * 2048 + (lane >> 2) * 16 + (lane & 3) * 4;
                         *reinterpret_cast<uint32_t *>(op + off) = pack2<E>(zr0, zr1);
-                        *reinterpret_cast<uint32_t *>(op + off + 8 * 2048) = pack2<E>(zi0, zi1);
+                        *reinterpret_cast<uint32_t *>(op + off + S::IM_OFF) = pack2<E>(zi0, zi1);
                     }
                 }
             } else {
 #pragma unroll
                 for (int j = 0; j < 8; ++j) {
-                    const int q = (j * 8 + warp) * 32 + lane;
+                    const int q = (j * W + warp) * 32 + lane;
                     const float4 hv = hreg[j];
                     const int d0 = (int)(dd[j] & 0xFFFFu), d1 = (int)(dd[j] >> 16);
 #pragma unroll
@@ -426,12 +461,12 @@ __global__ void __launch_bounds__(kThreads, 2) tc_dedisp_kernel(DedispArgs a)
                             const long long kk = kg + b;
                             // blocks before the stream start are zero
                             if (kk >= d0) {
-                                const float2 t = ring2[(size_t)((slot0 + b - d0) & smask) * kN + 2 * q];
+                                const float2 t = ring2[(size_t)((slot0 + b - d0) & smask) * N + 2 * q];
                                 x.x = t.x;
                                 x.y = t.y;
                             }
                             if (kk >= d1) {
-                                const float2 t = ring2[(size_t)((slot0 + b - d1) & smask) * kN + 2 * q + 1];
+                                const float2 t = ring2[(size_t)((slot0 + b - d1) & smask) * N + 2 * q + 1];
                                 x.z = t.x;
                                 x.w = t.y;
                             }
@@ -440,19 +475,22 @@ __global__ void __launch_bounds__(kThreads, 2) tc_dedisp_kernel(DedispArgs a)
                         const float zr1 = x.z * hv.z - x.w * hv.w, zi1 = x.z * hv.w + x.w * hv.z;
                         const int off = (b * 8 + j) * 128 + warp * 2048 + (lane >> 2) * 16 + (lane & 3) * 4;
                         *reinterpret_cast<uint32_t *>(op + off) = pack2<E>(zr0, zr1);
-                        *reinterpret_cast<uint32_t *>(op + off + 8 * 2048) = pack2<E>(zi0, zi1);
+                        *reinterpret_cast<uint32_t *>(op + off + S::IM_OFF) = pack2<E>(zi0, zi1);
                     }
                 }
             }
         };
 
-        // D1 -> twiddle (f16 arithmetic) -> f16 operand of GEMM 2 in `op`
-        // (rows 64 rb + m2, m2 = 32 h + 16 p + 8 g + 0..7; k = k1 (Re), 64 + k1 (Im))
+        // D1 -> twiddle (16-bit arithmetic) -> 16-bit operand of GEMM 2 in
+        // `op`: rows (N = 4096: 64 rb +) m2, m2 = 32 g + 16 p + 8 q + 0..7;
+        // k = k1 (Re), 64 + k1 (Im); at N = 8192 block rb's operand 32 KB on
         auto twiddle = [&](unsigned char *op) {
+            unsigned char *opb = op + (N2 == 64 ? 0 : 32768 * rb);
+            const int rg0 = N2 == 64 ? 8 * rb : 0;  // row group of m2 = 0
 #pragma unroll
             for (int p = 0; p < 2; ++p) {
                 float re[16], im[16];
-                tmem_ld_2x16(tD1 + 32 * h + 16 * p, tD1 + 64 + 32 * h + 16 * p, re, im);
+                tmem_ld_2x16(tD1 + 32 * g + 16 * p, tD1 + N2 + 32 * g + 16 * p, re, im);
                 uint32_t pr[8], pim[8];
 #pragma unroll
                 for (int i = 0; i < 8; ++i) {
@@ -465,52 +503,52 @@ __global__ void __launch_bounds__(kThreads, 2) tc_dedisp_kernel(DedispArgs a)
                     pim[i] = *reinterpret_cast<const uint32_t *>(&oi);
                 }
 #pragma unroll
-                for (int g = 0; g < 2; ++g) {
-                    const int off = (rb * 8 + 4 * h + 2 * p + g) * 128 + (ri >> 3) * 2048 + (ri & 7) * 16;
-                    st_shared_v4(op + off, pr[4 * g], pr[4 * g + 1], pr[4 * g + 2], pr[4 * g + 3]);
-                    st_shared_v4(op + off + 8 * 2048, pim[4 * g], pim[4 * g + 1], pim[4 * g + 2], pim[4 * g + 3]);
+                for (int q = 0; q < 2; ++q) {
+                    const int off = (rg0 + 4 * g + 2 * p + q) * 128 + (ri >> 3) * 2048 + (ri & 7) * 16;
+                    st_shared_v4(opb + off, pr[4 * q], pr[4 * q + 1], pr[4 * q + 2], pr[4 * q + 3]);
+                    st_shared_v4(opb + off + 8 * 2048, pim[4 * q], pim[4 * q + 1], pim[4 * q + 2], pim[4 * q + 3]);
                 }
             }
         };
 
-        // D2 -> outputs m = M + 64 c + m2 (c = 16 h + u) of pair i: series,
-        // detection into the intensity buffers (kM floats per block, in `op`)
+        // D2 -> outputs m = M + N2 c + m2 (c = 16 oh + u) of pair i: series,
+        // detection into the intensity buffers (M floats per block, in `op`)
         auto outputs = [&](int i, unsigned char *op) {
             const int k = kb + 2 * i;
             float yr[16], yi[16];
-            tmem_ld_2x16(tD2 + 16 * h, tD2 + 32 + 16 * h, yr, yi);
+            tmem_ld_2x16(tD2b + 16 * oh, tD2b + 32 + 16 * oh, yr, yi);
             if constexpr (SERIES) {
-                if (rb == 0 || k + 1 < ke) {
-                    float2 *out = a.series + (size_t)dm * a.count * kM + (size_t)(k + rb) * kM + 1024 * h + ri;
+                if (ob == 0 || k + 1 < ke) {
+                    float2 *out = a.series + (size_t)dm * a.count * M + (size_t)(k + ob) * M + 16 * N2 * oh + om2;
 #pragma unroll
                     for (int u = 0; u < 16; ++u)
-                        out[64 * u] = make_float2(yr[u] * isc, yi[u] * isc);
+                        out[N2 * u] = make_float2(yr[u] * isc, yi[u] * isc);
                 }
             }
             if constexpr (FOLD) {
-                float *ib = reinterpret_cast<float *>(op) + rb * kM + 1024 * h + ri;
+                float *ib = reinterpret_cast<float *>(op) + ob * M + 16 * N2 * oh + om2;
                 const float is2 = isc * isc;
                 if (a.fold.detect) {
 #pragma unroll
                     for (int u = 0; u < 16; ++u)
-                        ib[64 * u] = sqrtf((yr[u] * yr[u] + yi[u] * yi[u]) * is2);
+                        ib[N2 * u] = sqrtf((yr[u] * yr[u] + yi[u] * yi[u]) * is2);
                 } else {
 #pragma unroll
                     for (int u = 0; u < 16; ++u)
-                        ib[64 * u] = (yr[u] * yr[u] + yi[u] * yi[u]) * is2;
+                        ib[N2 * u] = (yr[u] * yr[u] + yi[u] * yi[u]) * is2;
                 }
             }
         };
 
         if (np > 0) {
             // prologue: pair 0 through GEMM 2's issue
-            unsigned char *opb = sm + kSmemOp0;
+            unsigned char *opb = sm + S::SMEM_OP0;
             gather(0, opb);
             fence_proxy_async();
             __syncthreads();
             if (tid == 0) {
                 tc_fence_after();
-                issue_cgemm<E>(tmem, s0 + kSmemOp0, s0 + kSmemB1, 64, barA);
+                issue_gemm1<E, LOG2N>(tmem, s0, s0 + S::SMEM_OP0, barA);
             }
             pendA = true;
             failed = !wait_gemm(tid, barA, phA);
@@ -522,12 +560,12 @@ __global__ void __launch_bounds__(kThreads, 2) tc_dedisp_kernel(DedispArgs a)
                 __syncthreads();
                 if (tid == 0) {
                     tc_fence_after();
-                    issue_cgemm<E>(tmem + 128, s0 + kSmemOp0, s0 + kSmemB2, 32, barB);
+                    issue_gemm2<E, LOG2N>(tmem, s0, s0 + S::SMEM_OP0, barB);
                 }
                 pendB = true;
             }
             for (int i = 0; i < np && !failed; ++i) {
-                const uint32_t cur = (i & 1) ? kSmemOp1 : kSmemOp0, nxt = (i & 1) ? kSmemOp0 : kSmemOp1;
+                const uint32_t cur = (i & 1) ? S::SMEM_OP1 : S::SMEM_OP0, nxt = (i & 1) ? S::SMEM_OP0 : S::SMEM_OP1;
                 const bool more = i + 1 < np;
                 if (more) {
                     // pair i + 1 into the other buffer; its GEMM 1 overlaps
@@ -537,7 +575,7 @@ __global__ void __launch_bounds__(kThreads, 2) tc_dedisp_kernel(DedispArgs a)
                     __syncthreads();
                     if (tid == 0) {
                         tc_fence_after();
-                        issue_cgemm<E>(tmem, s0 + nxt, s0 + kSmemB1, 64, barA);
+                        issue_gemm1<E, LOG2N>(tmem, s0, s0 + nxt, barA);
                     }
                     pendA = true;
                 }
@@ -552,10 +590,10 @@ __global__ void __launch_bounds__(kThreads, 2) tc_dedisp_kernel(DedispArgs a)
                     const int k = kb + 2 * i;
                     const float *ib0 = reinterpret_cast<const float *>(sm + cur);
                     __syncthreads();
-                    fold_block<false>(a.fold, fw, ib0, k * kM, kM, sp, sbase, scnt);
+                    fold_block<false>(a.fold, fw, ib0, k * M, M, sp, sbase, scnt);
                     if (k + 1 < ke) {
                         __syncthreads();
-                        fold_block<false>(a.fold, fw, ib0 + kM, (k + 1) * kM, kM, sp, sbase, scnt);
+                        fold_block<false>(a.fold, fw, ib0 + M, (k + 1) * M, M, sp, sbase, scnt);
                     }
                 }
                 if (more) {
@@ -570,7 +608,7 @@ __global__ void __launch_bounds__(kThreads, 2) tc_dedisp_kernel(DedispArgs a)
                     __syncthreads();
                     if (tid == 0) {
                         tc_fence_after();
-                        issue_cgemm<E>(tmem + 128, s0 + nxt, s0 + kSmemB2, 32, barB);
+                        issue_gemm2<E, LOG2N>(tmem, s0, s0 + nxt, barB);
                     }
                     pendB = true;
                 }
@@ -599,28 +637,36 @@ __global__ void __launch_bounds__(kThreads, 2) tc_dedisp_kernel(DedispArgs a)
         if (pendB)
             mbar_wait(barB, phB, kWaitLimitNs);
     }
-    tc_teardown(tmem, warp);
+    tc_teardown<LOG2N>(tmem, warp);
 }
 
 // One GEMM of the kernel on given data (layout check): A from a row-major
-// 128 x 128 f16 matrix, B the kernel's constant operand, D read back through
-// the kernel's tensor-memory view.
+// 128 x K 16-bit matrix, B the kernel's constant operand, D read back
+// through the kernel's tensor-memory view.  Step 1: GEMM 1 (K = 2 N2,
+// 2 N2 columns), step 2: GEMM 2 (K = 128, 64 columns).
+template <int LOG2N>
 __global__ void __launch_bounds__(kThreads, 1) tc_probe_kernel(int step, const uint16_t *A, float *D, int *status)
 {
+    using S = TcShape<LOG2N>;
     extern __shared__ __align__(1024) unsigned char sm[];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t s0 = smem_addr(sm);
-    const uint32_t bar = s0 + kSmemCtl;
-    fill_constants<F16>(sm, tid);
-    for (int e = tid; e < 128 * 128; e += kThreads) {
+    const uint32_t bar = s0 + S::SMEM_CTL;
+    const int kdim = step == 1 ? 2 * S::N2 : 128;
+    fill_constants<F16, LOG2N>(sm, tid);
+    for (int e = tid; e < 128 * kdim; e += blockDim.x) {
         const int r = e & 127, kk = e >> 7;
-        *reinterpret_cast<uint16_t *>(sm + kSmemOp0 + mn_off(r, kk)) = A[r * 128 + kk];
+        *reinterpret_cast<uint16_t *>(sm + S::SMEM_OP0 + mn_off(r, kk)) = A[r * kdim + kk];
     }
-    const uint32_t tmem = tc_setup(sm, s0, tid, warp);
-    const uint32_t tcol = step == 1 ? 0u : 128u;
+    const uint32_t tmem = tc_setup<LOG2N>(sm, s0, tid, warp);
+    const uint32_t tcol = step == 1 ? 0u : (uint32_t)S::D2_COL;
     if (tid == 0) {
         tc_fence_after();
-        issue_cgemm<F16>(tmem + tcol, s0 + kSmemOp0, s0 + (step == 1 ? kSmemB1 : kSmemB2), step == 1 ? 64 : 32, bar);
+        if (step == 1)
+            issue_cgemm<F16>(tmem, s0 + S::SMEM_OP0, s0 + S::SMEM_B1, S::N2, S::N2 / 16, S::SBO_B1);
+        else
+            issue_cgemm<F16>(tmem + tcol, s0 + S::SMEM_OP0, s0 + S::SMEM_B2, 32, 4, 1024);
+        mma_commit(bar);
     }
     uint32_t parity = 0;
     if (!wait_gemm(tid, bar, parity)) {
@@ -628,10 +674,10 @@ __global__ void __launch_bounds__(kThreads, 1) tc_probe_kernel(int step, const u
             atomicExch(status, 1);
             mbar_wait(bar, 0, kWaitLimitNs);
         }
-        tc_teardown(tmem, warp);
+        tc_teardown<LOG2N>(tmem, warp);
         return;
     }
-    const int ncol = step == 1 ? 128 : 64;
+    const int ncol = step == 1 ? 2 * S::N2 : 64;
     const int row = 32 * (warp & 3) + lane, h = warp >> 2;
     const uint32_t base = tmem + tcol + ((uint32_t)(32 * (warp & 3)) << 16);
     for (int c0 = h * ncol / 2; c0 < (h + 1) * ncol / 2; c0 += 32) {
@@ -642,105 +688,135 @@ __global__ void __launch_bounds__(kThreads, 1) tc_probe_kernel(int step, const u
             D[row * ncol + c0 + 16 + i] = y[i];
         }
     }
-    tc_teardown(tmem, warp);
+    tc_teardown<LOG2N>(tmem, warp);
 }
 
-__global__ void tc_permute_kernel(const float2 *__restrict__ in, float2 *__restrict__ out, long long n)
+__global__ void tc_permute_kernel(const float2 *__restrict__ in, float2 *__restrict__ out, long long n, int log2n)
 {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long nmask = (1ll << log2n) - 1;
     if (i < n)
-        out[(i & ~(long long)(kN - 1)) + tc_pos((int)(i & (kN - 1)))] = in[i];
+        out[(i & ~nmask) + tc_pos((int)(i & nmask), log2n)] = in[i];
 }
 
-template <class E, bool SERIES, bool FOLD>
-auto tc_fn() { return tc_dedisp_kernel<E, SERIES, FOLD>; }
+template <int LOG2N, class E, bool SERIES, bool FOLD>
+auto tc_fn() { return tc_dedisp_kernel<LOG2N, E, SERIES, FOLD>; }
 
-template <class E, typename G>
+template <int LOG2N, class E, typename G>
 auto tc_select_e(bool series, bool fold, G &&go)
 {
     if (series && fold)
-        return go(tc_fn<E, true, true>());
+        return go(tc_fn<LOG2N, E, true, true>());
     if (fold)
-        return go(tc_fn<E, false, true>());
-    return go(tc_fn<E, true, false>());
+        return go(tc_fn<LOG2N, E, false, true>());
+    return go(tc_fn<LOG2N, E, true, false>());
 }
 
-template <typename G>
-auto tc_select(bool bf16, bool series, bool fold, G &&go)
+template <int LOG2N, typename G>
+auto tc_select_n(bool bf16, bool series, bool fold, G &&go)
 {
     if (bf16)
-        return tc_select_e<BF16>(series, fold, go);
-    return tc_select_e<F16>(series, fold, go);
+        return tc_select_e<LOG2N, BF16>(series, fold, go);
+    return tc_select_e<LOG2N, F16>(series, fold, go);
 }
 
-}  // namespace
-
-bool tc_supported(int log2n) { return log2n == kLog2N; }
-
-size_t tc_smem_bytes(size_t extra) { return (size_t)kSmemFold + extra; }
-
-// Resident CTAs per SM from the shared-memory and register limits (at most
-// two: each CTA holds 256 of the SM's 512 tensor-memory columns).  The
-// occupancy API is not used here: it reports one CTA per SM for this kernel
-// where the hardware runs two.
-int tc_blocks_per_sm(bool bf16, bool series, bool fold, size_t extra_smem)
+template <int LOG2N>
+int tc_blocks_per_sm_t(bool bf16, bool series, bool fold, size_t extra_smem)
 {
-    const size_t sm = tc_smem_bytes(extra_smem);
-    int dev = 0, smem_sm = 0, reserved = 0, regs_sm = 0;
+    using S = TcShape<LOG2N>;
+    const size_t sm = (size_t)S::SMEM_FOLD + extra_smem;
+    int dev = 0, smem_sm = 0, reserved = 0, regs_sm = 0, smem_block = 0;
     if (cudaGetDevice(&dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&smem_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev) != cudaSuccess ||
+        cudaDeviceGetAttribute(&smem_block, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev) != cudaSuccess ||
         cudaDeviceGetAttribute(&regs_sm, cudaDevAttrMaxRegistersPerMultiprocessor, dev) != cudaSuccess)
         return 0;
-    return tc_select(bf16, series, fold, [&](auto k) -> int {
+    if (sm > (size_t)smem_block)
+        return 0;
+    return tc_select_n<LOG2N>(bf16, series, fold, [&](auto k) -> int {
         cudaFuncAttributes fa;
         if (cudaFuncGetAttributes(&fa, k) != cudaSuccess)
             return 0;
         const int by_smem = smem_sm / (int)(sm + (size_t)reserved);
-        const int regs_cta = ((fa.numRegs + 7) / 8) * 8 * kThreads;
+        const int regs_cta = ((fa.numRegs + 7) / 8) * 8 * S::THREADS;
         const int by_regs = regs_cta > 0 ? regs_sm / regs_cta : 0;
-        return std::min(2, std::min(by_smem, by_regs));
+        return std::min(S::CTAS_PER_SM, std::min(by_smem, by_regs));
     });
 }
 
-cudaError_t launch_tc_dedisp(bool bf16, bool series, bool fold, const DedispArgs &a, int grid, cudaStream_t st)
+template <int LOG2N>
+cudaError_t launch_tc_t(bool bf16, bool series, bool fold, const DedispArgs &a, int grid, cudaStream_t st)
 {
-    if (!a.status)
-        return cudaErrorInvalidValue;
-    const size_t sm =
-        tc_smem_bytes(fold ? fold_smem_bytes(a.fold.nbins, a.fold.span_cap, a.fold.smem_prof != 0, kThreads) : 0);
-    // at most two CTAs per SM (tensor memory: 256 of 512 columns each)
-    if (sm * 3 <= 228u * 1024u)
+    using S = TcShape<LOG2N>;
+    const size_t sm = (size_t)S::SMEM_FOLD +
+                      (fold ? fold_smem_bytes(a.fold.nbins, a.fold.span_cap, a.fold.smem_prof != 0, S::THREADS) : 0);
+    // no more CTAs per SM than the tensor memory holds (shared memory decides)
+    if (S::CTAS_PER_SM == 2 && sm * 3 <= 228u * 1024u)
         return cudaErrorInvalidConfiguration;
-    return tc_select(bf16, series, fold, [&](auto k) -> cudaError_t {
+    if (S::CTAS_PER_SM == 1 && sm * 2 <= 228u * 1024u)
+        return cudaErrorInvalidConfiguration;
+    return tc_select_n<LOG2N>(bf16, series, fold, [&](auto k) -> cudaError_t {
         cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e == cudaSuccess)
             e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
                                      (int)cudaSharedmemCarveoutMaxShared);
         if (e != cudaSuccess)
             return e;
-        k<<<grid, kThreads, sm, st>>>(a);
+        k<<<grid, S::THREADS, sm, st>>>(a);
         return cudaGetLastError();
     });
 }
 
-cudaError_t launch_tc_permute_rows(const float2 *in, float2 *out, int rows, cudaStream_t st)
+}  // namespace
+
+bool tc_supported(int log2n) { return log2n >= kLog2NMin && log2n <= kLog2NMax; }
+
+int tc_threads(int log2n) { return log2n == 13 ? TcShape<13>::THREADS : TcShape<12>::THREADS; }
+
+// Resident CTAs per SM from the shared-memory and register limits (the
+// tensor memory allows two at N = 4096, one at N = 8192); 0 when it does not
+// fit.  The occupancy API is not used: it reports one CTA per SM for the
+// 4096-point kernel where the hardware runs two.
+int tc_blocks_per_sm(int log2n, bool bf16, bool series, bool fold, size_t extra_smem)
 {
-    const long long n = (long long)rows * kN;
-    tc_permute_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(in, out, n);
+    if (log2n == 13)
+        return tc_blocks_per_sm_t<13>(bf16, series, fold, extra_smem);
+    return tc_blocks_per_sm_t<12>(bf16, series, fold, extra_smem);
+}
+
+cudaError_t launch_tc_dedisp(int log2n, bool bf16, bool series, bool fold, const DedispArgs &a, int grid,
+                             cudaStream_t st)
+{
+    if (!a.status || !tc_supported(log2n))
+        return cudaErrorInvalidValue;
+    if (log2n == 13)
+        return launch_tc_t<13>(bf16, series, fold, a, grid, st);
+    return launch_tc_t<12>(bf16, series, fold, a, grid, st);
+}
+
+cudaError_t launch_tc_permute_rows(const float2 *in, float2 *out, int rows, int log2n, cudaStream_t st)
+{
+    const long long n = (long long)rows << log2n;
+    tc_permute_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(in, out, n, log2n);
     return cudaGetLastError();
 }
 
 cudaError_t launch_tc_probe(int step, const uint16_t *a, float *d, int *status, cudaStream_t st)
 {
-    if (step != 1 && step != 2)
+    // steps 1, 2: the 4096-point GEMMs; step 3: the 8192-point GEMM 1
+    if (step < 1 || step > 3)
         return cudaErrorInvalidValue;
-    const size_t sm = kSmemFold;
-    cudaError_t e = cudaFuncSetAttribute(tc_probe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
-    if (e != cudaSuccess)
-        return e;
-    tc_probe_kernel<<<1, kThreads, sm, st>>>(step, a, d, status);
-    return cudaGetLastError();
+    auto run = [&](auto k, size_t sm, int st_) -> cudaError_t {
+        cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+        if (e != cudaSuccess)
+            return e;
+        k<<<1, kThreads, sm, st>>>(st_, a, d, status);
+        return cudaGetLastError();
+    };
+    if (step == 3)
+        return run(tc_probe_kernel<13>, (size_t)TcShape<13>::SMEM_FOLD, 1);
+    return run(tc_probe_kernel<12>, (size_t)TcShape<12>::SMEM_FOLD, step);
 }
 
 }  // namespace msosm

@@ -1,13 +1,13 @@
 // tc_layout.hpp -- data layout of the tensor-core (tcgen05) dedispersion path
-// for 4096-point transforms, shared by the host (set-up permutations) and the
-// device (kernels).
+// for 4096- and 8192-point transforms, shared by the host (set-up
+// permutations) and the device (kernels).
 //
-// The inverse 4096-point DFT is split as 64 x 64 (four-step): bin
-// k = k1 + 64 k2, output m = 64 m1 + m2,
-//   A[k1][m2]  = sum_k2 Z[k1 + 64 k2] e^{+2 pi i k2 m2 / 64}        (GEMM 1)
-//   A'[k1][m2] = A[k1][m2] e^{+2 pi i k1 m2 / 4096}                   (twiddle)
-//   y[64 m1 + m2] = sum_k1 A'[k1][m2] e^{+2 pi i k1 m1 / 64}, m1 >= 32 (GEMM 2)
-// Only m1 >= 32 (outputs m >= M = 2048) survive the overlap-save discard, so
+// The inverse N-point DFT is split as 64 x N2, N2 = N / 64 (four-step): bin
+// k = k1 + 64 k2, output m = N2 m1 + m2,
+//   A[k1][m2]  = sum_k2 Z[k1 + 64 k2] e^{+2 pi i k2 m2 / N2}          (GEMM 1)
+//   A'[k1][m2] = A[k1][m2] e^{+2 pi i k1 m2 / N}                      (twiddle)
+//   y[N2 m1 + m2] = sum_k1 A'[k1][m2] e^{+2 pi i k1 m1 / 64}, m1 >= 32 (GEMM 2)
+// Only m1 >= 32 (outputs m >= M = N / 2) survive the overlap-save discard, so
 // GEMM 2 computes half of its outputs.  Complex GEMMs run as real GEMMs:
 // with the data [Re | Im] (K = 128) and the DFT C + iS, the constant operand
 // holds only [C | S] (K = 64) and
@@ -18,8 +18,8 @@
 // f16 core matrices (8 rows of 16 contiguous bytes):
 //   data operand A (M = 128 rows x K = 128), MN-major: 8 consecutive rows of
 //     one K column are contiguous; row groups 128 B apart, K groups 2048 B
-//   constant operand B (N x K = 64), K-major: 8 consecutive K of one column
-//     contiguous; K groups 128 B apart, N groups 1024 B
+//   constant operand B (N x K), K-major: 8 consecutive K of one column
+//     contiguous; K groups 128 B apart, N groups K / 8 x 128 B apart
 #pragma once
 
 #include <cstdint>
@@ -28,39 +28,70 @@
 namespace msosm {
 namespace tc {
 
+// Shape of the tensor-core path for an N-point transform, N = 4096 or 8192:
+// bin k = k1 + 64 k2 (k1 < 64, k2 < N2 = N / 64), output m = N2 m1 + m2;
+// GEMM 1 sums over k2 (an N2-point DFT), GEMM 2 over k1 (64 points, m1 >= 32
+// kept).  At N = 4096 one GEMM 2 covers both blocks of a pair (rows 64 b +
+// m2); at N = 8192 each block has its own (rows m2 < 128).
+template <int LOG2N>
+struct TcShape {
+    static constexpr int N = 1 << LOG2N, M = N / 2;
+    static constexpr int N2 = N / 64;              // 64 or 128
+    static constexpr int WARPS = N2 / 8;           // 8 or 16
+    static constexpr int THREADS = 32 * WARPS;     // 256 or 512
+    static constexpr int CTAS_PER_SM = LOG2N == 12 ? 2 : 1;
+    static constexpr int B1_BYTES = 2 * N2 * N2 * 2;     // [C | S]: 2 N2 columns x N2 K, 16-bit
+    static constexpr int B2_BYTES = 64 * 64 * 2;         // [C | S]: 64 columns x 64 K
+    static constexpr int OP_BYTES = 128 * 2 * N2 * 2;    // GEMM 1 data operand (128 rows x 2 N2 K)
+    static constexpr int SMEM_B1 = 0;
+    static constexpr int SMEM_B2 = B1_BYTES;
+    static constexpr int SMEM_OP0 = B1_BYTES + B2_BYTES;  // two operand buffers; a buffer then
+    static constexpr int SMEM_OP1 = SMEM_OP0 + OP_BYTES;  // holds its pair's intensities
+    static constexpr int SMEM_CTL = SMEM_OP1 + OP_BYTES;  // mbarriers, TMEM address, per-warp maxima
+    static constexpr int SMEM_FOLD = SMEM_CTL + 256;      // fold span window, partials, profiles
+    static constexpr uint32_t SBO_B1 = (uint32_t)N2 * 16;  // B1 N-group stride (N2 / 8 K-groups x 128 B)
+    static constexpr int IM_OFF = (N2 / 8) * 2048;         // GEMM 1 operand: Im part, K = N2 on
+    static constexpr int D2_COL = 2 * N2;                  // TMEM: D1 at 0 .. 2 N2 - 1, D2 after it
+    static constexpr int TMEM_COLS = LOG2N == 12 ? 256 : 512;
+    static constexpr int SCALE_EXP = LOG2N == 12 ? 8 : 7;  // |Z| < 2^SCALE_EXP: GEMM 1 sums < 2^15
+};
+
+constexpr int kLog2NMin = 12, kLog2NMax = 13;
+// the 4096-point shape (also the GEMM layout check's)
 constexpr int kLog2N = 12;
 constexpr int kN = 1 << kLog2N, kM = kN / 2;
 constexpr int kThreads = 256;
+constexpr int kSmemB1 = TcShape<12>::SMEM_B1;
+constexpr int kSmemB2 = TcShape<12>::SMEM_B2;
+constexpr int kSmemOp0 = TcShape<12>::SMEM_OP0;
+constexpr int kSmemOp1 = TcShape<12>::SMEM_OP1;
+constexpr int kSmemCtl = TcShape<12>::SMEM_CTL;
+constexpr int kSmemFold = TcShape<12>::SMEM_FOLD;
+constexpr int kTmemCols = 256;
 
-// byte offsets in dynamic shared memory
-constexpr int kSmemB1 = 0;        // GEMM 1 constant [C | S]: 128 (N) x 64 (K) f16
-constexpr int kSmemB2 = 16384;    // GEMM 2 constant [C | S]:  64 (N) x 64 (K) f16
-constexpr int kSmemOp0 = 24576;   // two data-operand buffers (128 x 128 f16 each); a
-constexpr int kSmemOp1 = 57344;   //   buffer then holds its pair's intensities
-constexpr int kSmemCtl = 90112;   // mbarriers, TMEM address
-constexpr int kSmemFold = 90368;  // fold span window, partials and profiles
-constexpr int kTmemCols = 256;    // D1 at columns 0..127, D2 at 128..191
-
-// MN-major data operand: element (row r, k) -> byte offset
+// MN-major data operand (K groups 2048 B apart, row groups 128 B): element
+// (row r, k) -> byte offset
 __host__ __device__ constexpr int mn_off(int r, int k)
 {
     return (r >> 3) * 128 + (k >> 3) * 2048 + (k & 7) * 16 + (r & 7) * 2;
 }
-// K-major constant operand (K = 64): element (column n, k) -> byte offset
-__host__ __device__ constexpr int k_off(int n, int k)
+// K-major constant operand with N-group stride sbo: element (column n, k) -> byte offset
+__host__ __device__ constexpr int k_off(int n, int k, int sbo = 1024)
 {
-    return (n >> 3) * 1024 + (k >> 3) * 128 + (n & 7) * 16 + (k & 7) * 2;
+    return (n >> 3) * sbo + (k >> 3) * 128 + (n & 7) * 16 + (k & 7) * 2;
 }
 
-// Position of bin b in a tensor-core-ordered spectrum row (ring, H, delays).
-// Thread (warp w, lane l) of the gather reads, in pass j, the bin pair at
-// positions 64 (8 j + w) + 2 l + {0, 1}: bins k1 = 8 j + 2 (l & 3) + {0, 1},
-// k2 = 8 w + (l >> 2), which it stores as one 32-bit word of one core matrix
-// row -- a warp fills a whole 128-byte core matrix per store.
-__host__ __device__ constexpr int tc_pos(int b)
+// Position of bin b in a tensor-core-ordered spectrum row (ring, H, delays)
+// of N = 2^log2n points.  Thread (warp w, lane l) of the gather reads, in pass
+// j, the bin pair at positions 64 (W j + w) + 2 l + {0, 1} (W warps): bins
+// k1 = 8 j + 2 (l & 3) + {0, 1}, k2 = 8 w + (l >> 2), which it stores as one
+// 32-bit word of one core-matrix row -- a warp fills a whole 128-byte core
+// matrix per store.
+__host__ __device__ constexpr int tc_pos(int b, int log2n)
 {
     const int k1 = b & 63, k2 = b >> 6;
-    const int u = (k1 >> 3) * 8 + (k2 >> 3);
+    const int warps = (1 << (log2n - 6)) / 8;
+    const int u = (k1 >> 3) * warps + (k2 >> 3);
     const int l = (k2 & 7) * 4 + ((k1 & 7) >> 1);
     return u * 64 + l * 2 + (k1 & 1);
 }
@@ -75,11 +106,9 @@ __host__ __device__ constexpr uint64_t smem_desc(uint32_t addr, uint32_t lbo, ui
     return (uint64_t)((addr >> 4) & 0x3FFFu) | ((uint64_t)((lbo >> 4) & 0x3FFFu) << 16) |
            ((uint64_t)((sbo >> 4) & 0x3FFFu) << 32) | (1ull << 46);
 }
-// descriptor steps: K step of 16 f16 (two core-matrix columns) and the
-// constant operand's column offset
+// descriptor steps: K step of 16 elements (two core-matrix columns)
 constexpr uint32_t kDescStepA = 2 * 2048;  // MN-major data operand (LBO 2048, SBO 128)
-constexpr uint32_t kDescStepB = 2 * 128;   // K-major constant operand (LBO 128, SBO 1024)
-__host__ __device__ constexpr uint32_t b_col(int n) { return (uint32_t)(n >> 3) * 1024; }
+constexpr uint32_t kDescStepB = 2 * 128;   // K-major constant operand (LBO 128)
 
 // Instruction descriptor, kind::f16: f32 accumulator (bits 4-5 = 1), A and
 // B of one type (bits 7-9 and 10-12: 0 f16, 1 bf16), negate A (bit 13), A

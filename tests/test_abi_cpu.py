@@ -60,35 +60,40 @@ def test_tensor_path_rejects_other_fft_sizes():
     assert st == _abi.ERR_BAD_ARG and not h.value
 
 
-def test_tensor_layout_tables():
-    # host mirror of tc_pos (tc_layout.hpp) is a permutation of the 4096 bins,
-    # and the gather's thread mapping puts the bin pairs of one warp store in
-    # one 128-byte core matrix of the MN-major operand
+@pytest.mark.parametrize("log2n", [12, 13])
+def test_tensor_layout_tables(log2n):
+    # host mirror of tc_pos (tc_layout.hpp) is a permutation of the bins, and
+    # the gather's thread mapping (W warps) puts the bin pairs of one warp
+    # store in one 128-byte core matrix of the MN-major operand
+    N = 1 << log2n
+    W = (N // 64) // 8
+
     def tc_pos(b):
         k1, k2 = b & 63, b >> 6
-        u = (k1 >> 3) * 8 + (k2 >> 3)
+        u = (k1 >> 3) * W + (k2 >> 3)
         l = (k2 & 7) * 4 + ((k1 & 7) >> 1)
         return u * 64 + l * 2 + (k1 & 1)
 
     def mn_off(r, k):
         return (r >> 3) * 128 + (k >> 3) * 2048 + (k & 7) * 16 + (r & 7) * 2
 
-    pos = np.array([tc_pos(b) for b in range(4096)])
-    assert np.array_equal(np.sort(pos), np.arange(4096))
+    pos = np.array([tc_pos(b) for b in range(N)])
+    assert np.array_equal(np.sort(pos), np.arange(N))
     inv = np.argsort(pos)
     for j in range(8):
-        for w in range(8):
+        for w in range(W):
             offs = []
             for lane in range(32):
-                b = inv[(j * 8 + w) * 64 + 2 * lane]
+                b = inv[(j * W + w) * 64 + 2 * lane]
                 k1, k2 = b & 63, b >> 6
                 offs.append(mn_off(k1, k2))
-                assert inv[(j * 8 + w) * 64 + 2 * lane + 1] == b + 1
+                assert inv[(j * W + w) * 64 + 2 * lane + 1] == b + 1
             offs = np.array(offs)
             assert np.array_equal(np.sort(offs), offs.min() + 4 * np.arange(32))
             assert offs.min() % 128 == 0
-    # every operand element lies inside its 32 KB region
-    assert max(mn_off(r, k) for r in range(128) for k in range(128)) < 32768
+    # every operand element (128 rows, K = 2 N / 64) lies inside its buffer
+    K = 2 * (N // 64)
+    assert max(mn_off(r, k) for r in range(128) for k in range(K)) < 128 * K * 2
 
 
 @pytest.mark.parametrize("k", range(len(META["msosm"])))

@@ -31,24 +31,22 @@ def rel_rms(a, b):
 
 
 def dft_operand(step):
-    """The real form of the 64-point inverse DFT the kernel multiplies by,
-    K x N with K = [Re | Im] of the input index, rounded to float16."""
-    if step == 1:
-        k = np.arange(64)[:, None]
-        m = np.arange(64)[None, :]
-    else:
-        k = np.arange(64)[:, None]
-        m = np.arange(32, 64)[None, :]
-    ang = 2 * np.pi * ((k * m) % 64) / 64
+    """The real form of the inverse DFT the kernel multiplies by, K x N with
+    K = [Re | Im] of the input index, rounded to float16: step 1 the 64-point
+    DFT, step 2 its frequencies 32..63, step 3 the 128-point DFT."""
+    p = 128 if step == 3 else 64
+    k = np.arange(p)[:, None]
+    m = np.arange(32, 64)[None, :] if step == 2 else np.arange(p)[None, :]
+    ang = 2 * np.pi * ((k * m) % p) / p
     c, s = np.cos(ang), np.sin(ang)
     B = np.block([[c, s], [-s, c]])
     return B.astype(np.float16).astype(np.float64)
 
 
-@pytest.mark.parametrize("step", [1, 2])
+@pytest.mark.parametrize("step", [1, 2, 3])
 def test_gemm_layout_and_readback(step):
     rng = np.random.default_rng(step)
-    a = rng.standard_normal((128, 128)).astype(np.float16)
+    a = rng.standard_normal((128, 256 if step == 3 else 128)).astype(np.float16)
     d = tc_gemm_check(step, a)
     ref = a.astype(np.float64) @ dft_operand(step)
     err = np.max(np.abs(d - ref)) / np.max(np.abs(ref))
@@ -60,9 +58,9 @@ def u16(n, seed, scale=1000.0):
     return np.clip(np.rint(rng.standard_normal((n, 2)) * scale) + 32768, 1, 65535).astype(np.uint16)
 
 
-def run_pair(dms, count, calls, seed=0, series=True, x=None, precision="fp16"):
-    d = Dedisperser(BW, dms, F0, 4096, count, precision=precision, series=series)
-    o = O.Dedisp(BW, dms, F0, 4096, count)
+def run_pair(dms, count, calls, seed=0, series=True, x=None, precision="fp16", fft=4096):
+    d = Dedisperser(BW, dms, F0, fft, count, precision=precision, series=series)
+    o = O.Dedisp(BW, dms, F0, fft, count)
     if x is None:
         x = u16(d.block_samples * calls, seed)
     ours, ref = [], []
@@ -82,6 +80,18 @@ def test_series_matches_oracle(count, calls, precision):
     # the last block of a call unpaired
     dms = [0.0, 2.0, 5.0, 40.0, 100.0]
     ours, ref, _, _ = run_pair(dms, count, calls, seed=count, precision=precision)
+    for i in range(len(dms)):
+        e = rel_rms(ours[i], ref[i])
+        assert e < TOL[precision][0], (dms[i], e)
+
+
+@pytest.mark.parametrize("precision", ["fp16", "bf16"])
+@pytest.mark.parametrize("count,calls", [(4, 3), (3, 4)])
+def test_series_8192_matches_oracle(count, calls, precision):
+    # the 8192-point shape: 128-point GEMM 1, one GEMM 2 per block, 16 warps
+    dms = [0.0, 5.0, 60.0, 200.0]
+    ours, ref, d, _ = run_pair(dms, count, calls, seed=30 + count, precision=precision, fft=8192)
+    assert d.fftpoint == 8192
     for i in range(len(dms)):
         e = rel_rms(ours[i], ref[i])
         assert e < TOL[precision][0], (dms[i], e)
@@ -131,13 +141,13 @@ def test_full_scale_tone_stays_finite_and_accurate():
         assert rel_rms(ours[i], ref[i]) < SERIES_TOL
 
 
-@pytest.mark.parametrize("precision", ["fp16", "bf16"])
-def test_fold_matches_oracle(precision):
-    dms, count, calls, period, tb = [0.0, 20.0, 73.2], 8, 6, 0.0011, 256
-    d = Dedisperser(BW, dms, F0, 4096, count, series=False, precision=precision)
+@pytest.mark.parametrize("precision,fft", [("fp16", 4096), ("bf16", 4096), ("fp16", 8192)])
+def test_fold_matches_oracle(precision, fft):
+    dms, count, calls, period, tb = [0.0, 20.0, 73.2], 8 * 4096 // fft, 6, 0.0011, 256
+    d = Dedisperser(BW, dms, F0, fft, count, series=False, precision=precision)
     nd = 4096
     d.fold_init(period, BW, time_bin=tb, discard_Nd=nd)
-    o = O.Dedisp(BW, dms, F0, 4096, count)
+    o = O.Dedisp(BW, dms, F0, fft, count)
     x = u16(d.block_samples * calls, 21)
     ser = []
     for c in range(calls):
