@@ -9,7 +9,8 @@ FFT 4096 (MS-OSM, per-bin block delays), |y|^2 detection and folding into
 1024 phase bins per trial, all through libmsosm_b200.so.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference|reference-gpu]
-                    [--precision fp16|fp32]
+                    [--precision fp16|bf16|fp32]
+    python bench.py --workload precision-sweep [--seeds 8]
 
 The headline arm (default --precision fp16) runs the inverse transforms on
 the tensor cores (tcgen05 f16 GEMMs, f32 accumulation); the plain fused FP32
@@ -24,6 +25,13 @@ the timed region.  `--impl reference` times the oracle (the FP64 C
 restatement of the reference algorithm, OpenMP over trials) on the host
 cores on a bounded sample; `--impl reference-gpu` times the reference's own
 cuFFT classes built for sm_100a (oracle/_ref/ref_gpu_runner) when present.
+
+`--workload precision-sweep` (not the bench line): a 64 MHz band centred at
+1400 MHz, 2^26 samples, 1024 trials over 0-200, FFT 8192, with an injected
+pulsar (DM 150, P = 4.7 ms, 2% FWHM, peak SNR 0.05); per precision (FP32
+CUDA-core, FP16 and BF16 tensor-core) the device throughput, and for each of
+8 signal seeds the series and profile errors against the FP64 oracle on four
+sampled trials over the whole signal and the injected pulsar's S/N loss.
 """
 from __future__ import annotations
 
@@ -80,12 +88,20 @@ def dm_trials(rank, n_dm):
     return shard.weak_trials(rank, n_dm, DM_MAX)
 
 
-def make_signal(samples):
-    from msosm_gpu_b200 import simulate as S
+def make_signal(samples, on_gpu=True):
+    """The workload's baseband: the library's device simulator (counter-based
+    normals, overlap-save dispersion), or for the reference arms the host
+    generator (numpy), so that no code of this library runs on their path."""
     t = time.time()
-    x = S.pulsar_baseband(samples, BW, F0, PULSAR["dm"], PULSAR["period"], PULSAR["fwhm"], PULSAR["snr"],
-                          seed=PULSAR["seed"])
-    log(f"signal: {samples} samples generated in {time.time() - t:.1f} s")
+    if on_gpu:
+        from msosm_gpu_b200 import simulator as G
+        x = G.pulsar_baseband(samples, BW, F0, PULSAR["dm"], PULSAR["period"], PULSAR["fwhm"], PULSAR["snr"],
+                              seed=PULSAR["seed"])
+    else:
+        from msosm_gpu_b200 import simulate as S
+        x = S.pulsar_baseband(samples, BW, F0, PULSAR["dm"], PULSAR["period"], PULSAR["fwhm"], PULSAR["snr"],
+                              seed=PULSAR["seed"])
+    log(f"signal: {samples} samples generated in {time.time() - t:.1f} s ({'device' if on_gpu else 'host'})")
     return x
 
 
@@ -328,7 +344,7 @@ def run_ours(args):
     ms_max, tm, prof, clocks, nd_max = device_arm(args.precision, True)
     value = units / (ms_max * 1e-3) / 1e6
     peak_dm = float(dms[int(np.argmax(prof.max(1) - np.median(prof, 1)))])
-    other = "fp32" if args.precision == "fp16" else "fp16"
+    other = "fp16" if args.precision == "fp32" else "fp32"
     ms_o, tm_o, _, _, _ = device_arm(other, False)
     value_other = units / (ms_o * 1e-3) / 1e6
 
@@ -382,7 +398,7 @@ def run_ours(args):
         b = tr.get(key)
         return b * launch_samples if b else None
 
-    if args.precision == "fp16":
+    if args.precision in ("fp16", "bf16"):
         k_ms = tm["dedisp_ms"] / max(tm["calls"], 1)
         tpeak = peaks.get("bf16_tflops_sustained") or 1374.0
         ach = flops_per_sample * launch_samples / (k_ms * 1e-3) / 1e12
@@ -390,8 +406,8 @@ def run_ours(args):
         exec_tf = 2.0 * (128 * 128 * 128 + 128 * 64 * 128) / 4096.0 * launch_samples / (k_ms * 1e-3) / 1e12
         roofline = {"bound": "tensor", "achieved": ach, "peak": tpeak, "unit": "TFLOP/s", "frac": ach / tpeak,
                     "traffic": traffic_of("tc_bytes_per_dm_sample"),
-                    "kernel": "tc_dedisp_kernel (gather x H, inverse FFT as two tcgen05 f16 GEMMs + f16 twiddle, "
-                              "discard, |y|^2, fold)",
+                    "kernel": "tc_dedisp_kernel (gather x H, inverse FFT as two tcgen05 %s GEMMs + %s twiddle, "
+                              "discard, |y|^2, fold)" % (args.precision[:2] + "16", args.precision[:2] + "16"),
                     "flops_per_dm_sample": flops_per_sample, "kernel_ms": k_ms,
                     "executed_tensor_tflops": exec_tf, "executed_tensor_frac": exec_tf / tpeak,
                     "peak_source": "MEASURED_PEAKS.json bf16_tflops_sustained (f16 runs at the bf16 rate; the "
@@ -413,7 +429,8 @@ def run_ours(args):
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_max, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None,
-            "dtype": "f16 GEMM operands, f32 accumulation and gather" if args.precision == "fp16" else "f32",
+            "dtype": ("%s GEMM operands, f32 accumulation and gather" % (args.precision[:2] + "16")
+                      if args.precision != "fp32" else "f32"),
             "data": "synthetic (seeded pulsar + AWGN)",
             "config": dict(workload_config(samples, args.dms, ws), precision=args.precision),
             "e2e": {"value": e2e_v, "unit": UNIT, "h2d_bytes_per_step": int(x.nbytes),
@@ -440,6 +457,303 @@ def run_ours(args):
 
 
 # ---------------------------------------------------------------------------
+# precision sweep: 64 MHz band centred at 1400 MHz, FFT 8192, 1024 trials
+# ---------------------------------------------------------------------------
+
+SWEEP = dict(bw=64e6, f0=1368e6, fftpoint=8192, n_dm=1024, dm_max=200.0, log2_samples=26, nbins=1024,
+             pulsar=dict(dm=150.0, period=4.7e-3, fwhm=0.02, snr=0.05), seeds=8,
+             sample_dms=(0.0, 60.0, 150.0, 200.0), chunk_blocks=256)
+SWEEP_PRECS = ("fp32", "fp16", "bf16")
+
+
+def profile_snr(p, width):
+    """Boxcar matched-filter S/N of a folded profile: the largest circular
+    sum of ``width`` bins above the off-pulse mean, over the off-pulse
+    standard deviation times sqrt(width); off-pulse = every bin farther than
+    two widths from that window."""
+    p = np.asarray(p, np.float64)
+    n = p.size
+    c = np.concatenate([p, p[:width - 1]])
+    box = np.convolve(c, np.ones(width), "valid")[:n]
+    k = int(np.argmax(box))
+    mask = np.ones(n, bool)
+    mask[(np.arange(-2 * width, 3 * width) + k) % n] = False
+    off = p[mask]
+    return float((box[k] - width * off.mean()) / (off.std() * math.sqrt(width)))
+
+
+def sweep_throughput(x, dms, steps, warmup):
+    """Device time of one step (all samples, all trials, fold only) for each
+    precision, input resident in HBM."""
+    import torch
+    from msosm_gpu_b200 import Dedisperser
+    cfg = SWEEP
+    M = cfg["fftpoint"] // 2
+    xd = torch.from_numpy(x).cuda()
+    stream = torch.cuda.Stream()
+    out = {}
+    for prec in SWEEP_PRECS:
+        d = Dedisperser(cfg["bw"], dms, cfg["f0"], cfg["fftpoint"], count=x.size // M, series=False,
+                        precision=prec)
+        d.set_stream(stream)
+        d.fold_init(cfg["pulsar"]["period"], cfg["bw"], time_bin=cfg["nbins"], discard_Nd=int(d.Nd.max()),
+                    detect="power")
+        for _ in range(warmup):
+            d.filter_block(xd)
+        torch.cuda.synchronize()
+        d.enable_timing(True)
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            s.record(stream)
+            for _ in range(steps):
+                d.filter_block(xd)
+            e.record(stream)
+        torch.cuda.synchronize()
+        ms = s.elapsed_time(e) / steps
+        tm = d.timing()
+        c = max(tm["calls"], 1)
+        prof = d.get_profiles()
+        width = max(1, int(round(cfg["pulsar"]["fwhm"] * cfg["nbins"])))
+        snr = np.array([profile_snr(p, width) for p in prof])
+        out[prec] = {"ms_per_step": ms, "value": len(dms) * x.size / (ms * 1e-3) / 1e6,
+                     "stage_ms_per_step": {"forward": tm["forward_ms"] / c, "dedisp": tm["dedisp_ms"] / c,
+                                           "fold": tm["fold_ms"] / c},
+                     "best_trial_dm": float(dms[int(np.argmax(snr))]), "best_trial_snr": float(snr.max())}
+        d.close()
+    del xd
+    return out
+
+
+def sweep_accuracy(x, seed):
+    """Errors of the three device precisions against the FP64 oracle for the
+    sampled trials over the whole signal (chunked calls): dedispersed series
+    and folded |y|^2 profiles, and the injected pulsar's S/N in each
+    precision's profile relative to the oracle's."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    from msosm_gpu_b200 import Dedisperser
+    cfg = SWEEP
+    threads = os.cpu_count() or 1
+    O.lib().orc_set_threads(threads)
+    dms = np.array(cfg["sample_dms"], np.float32)
+    count = cfg["chunk_blocks"]
+    o = O.Dedisp(cfg["bw"], dms, cfg["f0"], cfg["fftpoint"], count, threads=threads)
+    blk = count * o.M
+    nd = int(max(o.Nd))
+    devs = {}
+    for prec in SWEEP_PRECS:
+        dv = Dedisperser(cfg["bw"], dms, cfg["f0"], cfg["fftpoint"], count=count, precision=prec)
+        dv.fold_init(cfg["pulsar"]["period"], cfg["bw"], time_bin=cfg["nbins"], discard_Nd=nd, detect="power")
+        devs[prec] = dv
+    folds = [O.Fold(cfg["pulsar"]["period"], cfg["bw"], blk, cfg["nbins"]) for _ in dms]
+    for f in folds:
+        f.discard_samples(nd)
+    ref2 = np.zeros(len(dms))
+    err2 = {p: np.zeros(len(dms)) for p in devs}
+    emax = {p: np.zeros(len(dms)) for p in devs}
+    calls = x.size // blk
+    for c in range(calls):
+        seg = np.ascontiguousarray(x[c * blk:(c + 1) * blk])
+        y = o.filter(seg.astype(np.complex128))
+        ref2 += np.sum(np.abs(y) ** 2, axis=1)
+        for i, f in enumerate(folds):
+            f.fold_data(np.abs(y[i]) ** 2)
+        for p, dv in devs.items():
+            dv.filter_block(seg)
+            e = np.abs(dv.get_output().astype(np.complex128) - y)
+            err2[p] += np.sum(e * e, axis=1)
+            emax[p] = np.maximum(emax[p], e.max(axis=1))
+    pref = np.stack([f.fold_data_bins() for f in folds])
+    width = max(1, int(round(cfg["pulsar"]["fwhm"] * cfg["nbins"])))
+    inj = int(np.argmin(np.abs(dms - cfg["pulsar"]["dm"])))
+    snr_ref = profile_snr(pref[inj], width)
+    rms_ref = np.sqrt(ref2 / (calls * blk))
+    res = {"seed": seed, "snr_fp64": snr_ref}
+    for p, dv in devs.items():
+        prof = dv.get_profiles().astype(np.float64)
+        dp = prof - pref
+        snr = profile_snr(prof[inj], width)
+        res[p] = {"series_rel_rms": (np.sqrt(err2[p] / np.maximum(ref2, 1e-300))).tolist(),
+                  "series_max_abs_over_rms": (emax[p] / np.maximum(rms_ref, 1e-300)).tolist(),
+                  "profile_rel_rms": (np.sqrt(np.sum(dp ** 2, 1) / np.sum(pref ** 2, 1))).tolist(),
+                  "profile_max_abs_over_mean": (np.abs(dp).max(1) / np.abs(pref).mean(1)).tolist(),
+                  "snr": snr, "snr_loss": 1.0 - snr / snr_ref}
+        dv.close()
+    return res
+
+
+def run_precision_sweep(args):
+    from msosm_gpu_b200 import simulator as G
+    cfg = SWEEP
+    samples = 1 << (args.log2_samples or cfg["log2_samples"])
+    n_dm = args.dms or cfg["n_dm"]
+    dms = np.linspace(0.0, cfg["dm_max"], n_dm).astype(np.float32)
+    pul = cfg["pulsar"]
+
+    def signal(seed):
+        t = time.time()
+        x = G.pulsar_baseband(samples, cfg["bw"], cfg["f0"], pul["dm"], pul["period"], pul["fwhm"], pul["snr"],
+                              seed=seed)
+        log(f"seed {seed}: {samples} samples generated in {time.time() - t:.1f} s")
+        return x
+
+    x = signal(0)
+    thr = sweep_throughput(x, dms, args.steps, args.warmup)
+    log("throughput: " + json.dumps(thr))
+    seeds = []
+    for seed in range(args.seeds):
+        if seed:
+            x = signal(seed)
+        t = time.time()
+        seeds.append(sweep_accuracy(x, seed))
+        log(f"seed {seed}: accuracy in {time.time() - t:.1f} s: " + json.dumps(seeds[-1]))
+    summary = {}
+    for p in SWEEP_PRECS:
+        def agg(key):
+            v = np.array([r[p][key] for r in seeds], np.float64)
+            return {"median": float(np.median(v)), "max": float(v.max())} if v.size else None
+        summary[p] = {"series_rel_rms": agg("series_rel_rms"),
+                      "series_max_abs_over_rms": agg("series_max_abs_over_rms"),
+                      "profile_rel_rms": agg("profile_rel_rms"),
+                      "profile_max_abs_over_mean": agg("profile_max_abs_over_mean"),
+                      "snr_loss": agg("snr_loss"),
+                      "throughput": thr[p]["value"], "ms_per_step": thr[p]["ms_per_step"],
+                      "speedup_vs_fp32": thr[p]["value"] / thr["fp32"]["value"]}
+    line = {"workload": "tensor-core precision sweep: 64 MHz band centred at 1400 MHz (f0 1368 MHz), "
+                        "2^%d complex64 samples, %d DM trials 0-%g, FFT %d, fold %d bins"
+                        % (int(math.log2(samples)), n_dm, cfg["dm_max"], cfg["fftpoint"], cfg["nbins"]),
+            "unit": UNIT, "data": "synthetic (seeded pulsar + AWGN)",
+            "pulsar": pul, "seeds": args.seeds, "steps": args.steps, "warmup": args.warmup,
+            "precisions": {"fp32": "FP32 CUDA-core inverse FFT (the plain fused path)",
+                           "fp16": "tcgen05 f16 operands, f32 accumulation",
+                           "bf16": "tcgen05 bf16 operands, f32 accumulation",
+                           "split_hi_lo": "not built"},
+            "error_reference": "FP64 oracle (oracle/orc.c: the reference algorithm in double precision, "
+                               "radix-2 FFT; FFTW is not available)",
+            "error_sample": "trials %s over every sample of each seed's signal (calls of %d blocks); series "
+                            "error relative to the oracle's RMS, profile error relative to the oracle's "
+                            "profile; S/N by a %d-bin boxcar at the trial nearest the injected DM"
+                            % (list(cfg["sample_dms"]), cfg["chunk_blocks"],
+                               max(1, int(round(pul["fwhm"] * cfg["nbins"])))),
+            "throughput_sample": "seed 0, all trials, device time per step (CUDA events), input resident in HBM",
+            "summary": summary, "throughput": thr, "per_seed": seeds}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# uneven batch: 64 independent observations, autotuned against fixed choices
+# ---------------------------------------------------------------------------
+
+UNEVEN = dict(n_obs=64, log2_len=(20, 25), bws=(4e6, 16e6, 32e6, 64e6), centre=(1100e6, 1500e6),
+              trials=(16, 512), dm_max=(20.0, 300.0), period=(1e-3, 1.0), duty=(0.01, 0.10),
+              snr=(0.02, 0.2), nbins=256, seed=0)
+FIXED = [(2048, "fp32"), (4096, "fp32"), (8192, "fp32"), (16384, "fp32"), (32768, "fp32"), (4096, "fp16"),
+         (8192, "fp16")]
+
+
+def uneven_observations(n_obs, seed):
+    """The observations' parameters: lengths log-uniform 2^20 .. 2^25 (whole
+    multiples of 2^15 samples), bandwidth from {4, 16, 32, 64} MHz, centre
+    uniform 1100 .. 1500 MHz, trial counts log-uniform 16 .. 512 over
+    0 .. DM_max with DM_max uniform 20 .. 300, one pulsar each (period
+    log-uniform 1 ms .. 1 s, duty cycle 1 .. 10 %, peak SNR 0.02 .. 0.2, DM
+    uniform over the middle 80 % of the range, lowered where the simulator's
+    dispersion filter would pass 2^24 points)."""
+    from msosm_gpu_b200.autotune import log_uniform
+    from msosm_gpu_b200.prepare import nd, osm_min_order
+    cfg = UNEVEN
+    rng = np.random.default_rng(seed)
+    obs = []
+    for i in range(n_obs):
+        n = int(2 ** rng.uniform(*cfg["log2_len"])) // (1 << 15) * (1 << 15)
+        bw = float(cfg["bws"][rng.integers(len(cfg["bws"]))])
+        f0 = float(np.float32(rng.uniform(*cfg["centre"]) - bw / 2))
+        D = int(round(log_uniform(rng, *cfg["trials"])))
+        dm_max = float(rng.uniform(*cfg["dm_max"]))
+        dm = float(rng.uniform(0.1, 0.9) * dm_max)
+        while 2 * osm_min_order(nd(bw, dm, f0)) > (1 << 24):
+            dm *= 0.8
+        obs.append(dict(i=i, n=n, bw=bw, f0=f0, trials=D, dm_max=dm_max, dm=dm,
+                        period=log_uniform(rng, *cfg["period"]), duty=float(rng.uniform(*cfg["duty"])),
+                        snr=float(rng.uniform(*cfg["snr"]))))
+    return obs
+
+
+def run_uneven_batch(args):
+    import torch
+    from msosm_gpu_b200 import Dedisperser
+    from msosm_gpu_b200 import simulator as G
+    from msosm_gpu_b200.autotune import Autotuner, fixed_choice
+    cfg = UNEVEN
+    obs = uneven_observations(args.obs, cfg["seed"])
+    tuner = Autotuner(sample=1 << 21, calls=2)
+    stream = torch.cuda.Stream()
+    times = []   # per observation: {(fft, prec): ms}
+    tuned, tuning_s, detect = [], 0.0, []
+    total_units = 0.0
+    for o in obs:
+        dms = np.linspace(0.0, o["dm_max"], o["trials"]).astype(np.float32)
+        t = time.time()
+        ch = tuner.tune(o["bw"], dms, o["f0"], period=o["period"], time_bin=cfg["nbins"])
+        tuning_s += time.time() - t
+        tuned.append((ch.fftpoint, ch.precision))
+        x = G.pulsar_baseband(o["n"], o["bw"], o["f0"], o["dm"], o["period"], o["duty"], o["snr"], seed=o["i"],
+                              device=torch.device("cuda"))
+        need = {(ch.fftpoint, ch.precision)} | {fixed_choice(o["bw"], dms, o["f0"], n, p) for n, p in FIXED}
+        res = {}
+        for n, p in sorted(need):
+            d = Dedisperser(o["bw"], dms, o["f0"], n, count=o["n"] // (n // 2), series=False, precision=p)
+            d.set_stream(stream)
+            d.fold_init(o["period"], o["bw"], time_bin=cfg["nbins"], discard_Nd=int(d.Nd.max()), detect="power")
+            torch.cuda.synchronize()
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(stream):
+                s.record(stream)
+                d.filter_block(x)
+                e.record(stream)
+            torch.cuda.synchronize()
+            res[(n, p)] = s.elapsed_time(e)
+            if (n, p) == (ch.fftpoint, ch.precision) and d.folded_periods() >= 8:
+                prof = d.get_profiles().astype(np.float64)
+                w = max(1, int(round(o["duty"] * cfg["nbins"])))
+                snr = np.array([profile_snr(q, w) for q in prof])
+                step = o["dm_max"] / max(o["trials"] - 1, 1)
+                detect.append(abs(float(dms[int(np.argmax(snr))]) - o["dm"]) <= 1.5 * step)
+            d.close()
+        del x
+        times.append(res)
+        total_units += o["trials"] * o["n"]
+        log(f"obs {o['i']}: n={o['n']} bw={o['bw'] / 1e6:g} D={o['trials']} dm_max={o['dm_max']:.0f} "
+            f"tuned={ch.fftpoint}/{ch.precision} " + " ".join(f"{k[0]}/{k[1]}={v:.1f}" for k, v in sorted(res.items())))
+    tuned_ms = sum(r[c] for r, c in zip(times, tuned))
+    fixed = {}
+    for n, p in FIXED:
+        ms = 0.0
+        for o, r in zip(obs, times):
+            dms = np.linspace(0.0, o["dm_max"], o["trials"]).astype(np.float32)
+            ms += r[fixed_choice(o["bw"], dms, o["f0"], n, p)]
+        fixed[f"{n}/{p}"] = {"ms": ms, "value": total_units / (ms * 1e-3) / 1e6}
+    best = max(fixed, key=lambda k: fixed[k]["value"])
+    tuned_v = total_units / (tuned_ms * 1e-3) / 1e6
+    line = {"workload": "uneven batch: %d independent observations (lengths 2^20-2^25, bandwidth 4/16/32/64 MHz, "
+                        "centre 1100-1500 MHz, 16-512 trials over 0-DM_max, DM_max 20-300), one injected pulsar "
+                        "each, fold %d bins" % (len(obs), cfg["nbins"]),
+            "unit": UNIT, "data": "synthetic (device simulator, seeded)",
+            "method": "each observation one filter_block call on device-resident input, CUDA events on the "
+                      "handle's stream; fixed configurations raise the FFT to an observation's minimum and "
+                      "fall back to FP32 where the tensor path has no kernel; the autotuner times every "
+                      "candidate on 2^21 samples of noise per observation shape",
+            "total_dm_trial_samples": total_units,
+            "tuned": {"ms": tuned_ms, "value": tuned_v,
+                      "choices": {f"{n}/{p}": tuned.count((n, p)) for n, p in sorted(set(tuned))}},
+            "fixed": fixed, "best_fixed": best, "tuned_vs_best_fixed": tuned_v / fixed[best]["value"],
+            "tuning_s": tuning_s,
+            "detected": {"eligible": len(detect), "within_1.5_trial_steps": int(sum(detect))},
+            "observations": obs}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
 # reference arms
 # ---------------------------------------------------------------------------
 
@@ -449,7 +763,7 @@ def run_reference(args):
         return
     samples = 1 << args.log2_samples
     dms = dm_trials(0, args.dms)
-    x = make_signal(min(samples, 1 << 22))
+    x = make_signal(min(samples, 1 << 22), on_gpu=False)
     vals, cb = [], None
     for _ in range(args.warmup + args.steps):
         cb = cpu_baseline(dms, x, budget_s=max(2.0, 60.0 / max(args.steps, 1)))
@@ -478,7 +792,7 @@ def run_reference_gpu(args):
     samples = 1 << args.log2_samples
     # the reference leaves delays uninitialised at DM 0: trials (0, 100]
     dms = ((np.arange(args.dms) + 1) * DM_MAX / args.dms).astype(np.float32)
-    x = make_signal(samples)
+    x = make_signal(samples, on_gpu=False)
     u = S.quantise_uint16(x, 1000.0)
     count = 32
     ncalls = samples // (count * FFTPOINT // 2)
@@ -515,12 +829,27 @@ def main():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference", "reference-gpu"])
-    ap.add_argument("--log2-samples", type=int, default=LOG2_SAMPLES)
-    ap.add_argument("--dms", type=int, default=N_DM)
+    ap.add_argument("--log2-samples", type=int, default=None, help="default 26 for both workloads")
+    ap.add_argument("--dms", type=int, default=None, help="default 256 (batched) or 1024 (precision-sweep)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--precision", default="fp16", choices=["fp32", "fp16"],
-                    help="inverse transforms on the CUDA cores (fp32) or the tensor cores (fp16)")
+    ap.add_argument("--precision", default="fp16", choices=["fp32", "fp16", "bf16"],
+                    help="inverse transforms on the CUDA cores (fp32) or the tensor cores (fp16, bf16)")
+    ap.add_argument("--workload", default="batched", choices=["batched", "precision-sweep", "uneven-batch"],
+                    help="batched: the 256-trial 16 MHz workload (the bench line); precision-sweep: the "
+                         "64 MHz / FFT 8192 / 1024-trial sweep of the inverse-transform precisions; "
+                         "uneven-batch: 64 independent observations, autotuned vs fixed configurations")
+    ap.add_argument("--obs", type=int, default=UNEVEN["n_obs"], help="uneven-batch: observations")
+    ap.add_argument("--seeds", type=int, default=SWEEP["seeds"], help="precision-sweep: signal seeds")
     args = ap.parse_args()
+    if args.workload != "batched":
+        if args.impl != "ours":
+            print(json.dumps({"impl": args.impl, "unavailable": f"the {args.workload} workload has no "
+                              "reference arm"}))
+            return
+        (run_precision_sweep if args.workload == "precision-sweep" else run_uneven_batch)(args)
+        return
+    args.log2_samples = args.log2_samples or LOG2_SAMPLES
+    args.dms = args.dms or N_DM
     if args.impl == "reference":
         run_reference(args)
     elif args.impl == "reference-gpu":

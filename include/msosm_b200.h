@@ -132,6 +132,12 @@ typedef struct msosm_dedisp msosm_dedisp;
 /* As MSOSM_FLAG_TENSOR_F16 with bf16 operands (no scaling needed; relative
  * RMS error of the series against FP64 about 4e-3). */
 #define MSOSM_FLAG_TENSOR_BF16 0x8u
+/* With MSOSM_FLAG_OSM only: the filter designed from the +phase chirp, the
+ * dispersion filter of the reference's signal simulator
+ * (simulated_pulsar/simulated_complex_signal.cpp:91-107), instead of the
+ * dedispersion filter; the output is half the dispersed input, delayed by
+ * M - Nd samples at the top of the band. */
+#define MSOSM_FLAG_DISPERSE 0x10u
 
 typedef struct msosm_dedisp_info {
     unsigned long M;        /* hop / filter order; FFT size is 2M */
@@ -328,6 +334,95 @@ MSOSM_API msosm_status msosm_dada_read_count(const msosm_dada *d, unsigned long 
  * than 2n samples are left (the reference reads past the end silently). */
 MSOSM_API msosm_status msosm_dada_read(msosm_dada *d, unsigned long n, msosm_uint16_pair *pol1,
                                        msosm_uint16_pair *pol2);
+
+/* ======================================================================
+ * Signal simulator (simulated_pulsar/) and host buffers
+ * ====================================================================== */
+
+/* Host memory for signals: pinned (cudaMallocHost, as the reference's
+ * generate_pulsar_signal(pinned = true) allocates) or plain malloc. */
+MSOSM_API msosm_status msosm_host_alloc(size_t bytes, int pinned, void **out);
+MSOSM_API msosm_status msosm_host_free(void *p, int pinned);
+
+/* Random numbers of every simulator: Philox4x32-10 (Salmon et al., SC11,
+ * 2011) at counter (lo(i), hi(i), tag, 0) under the key (lo(seed), hi(seed))
+ * for sample i; Box-Muller in double precision turns the block's four words
+ * into two complex unit normals (variance 1 per component) rounded to float.
+ * A sample's numbers depend only on (seed, i, tag).  Tags: 0 the pulsar
+ * generator (z1: emission, z2: system noise), 1 AWGN. */
+#define MSOSM_SIM_TAG_PULSAR 0u
+#define MSOSM_SIM_TAG_AWGN 1u
+/* z1[j], z2[j] of samples i = start + j, j < n (either may be NULL; host or
+ * device pointers).  Needs a GPU. */
+MSOSM_API msosm_status msosm_sim_normals(unsigned long long seed, unsigned long long start, unsigned long n,
+                                         unsigned int tag, msosm_complex *z1, msosm_complex *z2);
+
+/* AWGN::generateNoiseSamples (simulated_pulsar/AWGN.cpp:29-58) with the
+ * tag-1 normals z of `seed`: snr_mode 1 (AWGN(SNR, n)) gives
+ * sigma / sqrt(2) * z, sigma = sqrt(10^(-SNR/10)); snr_mode 0 (AWGN(mean,
+ * variance, n)) gives z * variance + mean (the reference passes the variance
+ * as the standard deviation).  The reference's default-seeded
+ * std::default_random_engine sequence is not reproduced. */
+MSOSM_API msosm_status msosm_sim_awgn(unsigned long long seed, unsigned long n, int snr_mode, float mean,
+                                      float variance, float snr_db, msosm_complex *out);
+
+/* SimulatedComplexSignal's sizes (simulated_complex_signal.cpp:21-25,
+ * 52-71): Np = period samples, Nd = dispersion smear, range =
+ * ceil(Nd / Np) periods (at least 1), order = 2^ceil(log2(range Np)). */
+typedef struct msosm_sim_two_spike_info {
+    unsigned long Np, Nd, range, order;
+} msosm_sim_two_spike_info;
+MSOSM_API msosm_status msosm_sim_two_spike_shape(float bw, float dm, float f0, float period,
+                                                msosm_sim_two_spike_info *info);
+/* SimulatedComplexSignal(bw, dm, f0, period).generate_pulsar_signal(repeat,
+ * add_noise, SNR) (simulated_complex_signal.cpp:40-236) on the device: one
+ * period of two unit deltas at Np/2 and Np/2 + 2 dispersed by the +phase
+ * chirp filter of `order` points and summed over `range` periods, tiled
+ * `repeat` times; with add_noise, AWGN at SNR dB relative to the period's
+ * measured power (tag-1 normals of `seed`).  signal: repeat * Np complex;
+ * signal_u16: the reference's codec ((v == 0) ? 0 : uint16(v * 32767 +
+ * 32768), wrapping); signal_power_db: the measured power.  Outputs may be
+ * NULL, host or device.  order 64 .. 2^24. */
+MSOSM_API msosm_status msosm_sim_two_spike(float bw, float dm, float f0, float period, unsigned long repeat,
+                                           int add_noise, float snr_db, unsigned long long seed,
+                                           msosm_complex *signal, msosm_uint16_pair *signal_u16,
+                                           float *signal_power_db);
+
+/* Streaming noisy pulsar: x(t) = D[a z1](t) + z2(t) / sqrt(2), t = 0, 1, ...,
+ * a(t) = sqrt(snr g(phase)) / sqrt(2), g a Gaussian profile of peak 1 and
+ * FWHM `fwhm` (fraction of the period) centred at phase `centre`, phase =
+ * frac(t / bw / period), z1 and z2 the tag-0 normals, D the overlap-save
+ * dispersion filter (MSOSM_FLAG_OSM | MSOSM_FLAG_DISPERSE, order 2 *
+ * nextpow2(Nd); none at Nd = 0).  The pulsar/noise power ratio peaks at snr.
+ * The dispersion filter is causal: the emission at t arrives between
+ * t + M - Nd (top of the band) and t + M (bottom), M its order. */
+typedef struct msosm_sim_pulsar_params {
+    float bw;       /* Hz (complex sampling rate) */
+    float f0;       /* lower band edge, Hz */
+    float dm;       /* pc cm^-3 */
+    double period;  /* s */
+    double fwhm;    /* pulse FWHM, fraction of the period */
+    double centre;  /* pulse centre phase */
+    double snr;     /* peak pulsar/noise power ratio per sample */
+    unsigned long long seed;
+} msosm_sim_pulsar_params;
+typedef struct msosm_sim msosm_sim;
+typedef struct msosm_sim_pulsar_info {
+    unsigned long chunk;            /* samples per msosm_sim_pulsar_next */
+    unsigned long M;                /* dispersion filter order (0: none) */
+    unsigned long Nd;               /* dispersion smear, samples */
+    unsigned long long next_sample; /* index of the next chunk's first sample */
+} msosm_sim_pulsar_info;
+/* chunk = min_chunk rounded up to a multiple of M (0: 2^22). */
+MSOSM_API msosm_status msosm_sim_pulsar_create(const msosm_sim_pulsar_params *p, unsigned long min_chunk,
+                                               msosm_sim **out);
+MSOSM_API msosm_status msosm_sim_pulsar_destroy(msosm_sim *s);
+MSOSM_API msosm_status msosm_sim_pulsar_get_info(const msosm_sim *s, msosm_sim_pulsar_info *info);
+/* The next chunk samples: complex (out) and/or offset-binary uint16 pairs of
+ * rint(x * u16_scale) + 32768 clipped to 1 .. 65535 (u16); host or device
+ * pointers, either may be NULL. */
+MSOSM_API msosm_status msosm_sim_pulsar_next(msosm_sim *s, msosm_complex *out, msosm_uint16_pair *u16,
+                                             double u16_scale);
 
 /* ======================================================================
  * Diagnostics (no counterpart in the reference)

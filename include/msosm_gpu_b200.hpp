@@ -563,4 +563,114 @@ private:
     std::vector<uint16_pair> pol1_, pol2_;
 };
 
+// ---------------------------------------------------------------------------
+// simulated_pulsar/include/AWGN.h:8-31 -- complex white Gaussian noise
+// (msosm_sim_awgn).  `seed` replaces the reference's default-seeded engine.
+// ---------------------------------------------------------------------------
+
+class AWGN {
+public:
+    AWGN() : mean(0.f), variance(1.f), numberOfSamples(100), isSNRMode(false) {}
+    AWGN(float mean_, float variance_, unsigned long n)
+        : mean(mean_), variance(variance_), numberOfSamples(n), isSNRMode(false)
+    {
+    }
+    AWGN(float SNR, unsigned long n) : mean(0.f), variance(1.f), numberOfSamples(n), isSNRMode(true), snr(SNR) {}
+    AWGN(const AWGN &) = delete;
+    AWGN &operator=(const AWGN &) = delete;
+    ~AWGN() { deallocate(); }
+
+    // numberOfSamples complex values in host memory owned by this object
+    // until deallocate()
+    Complex *generateNoiseSamples()
+    {
+        deallocate();
+        check(msosm_host_alloc(sizeof(Complex) * numberOfSamples, 0, (void **)&samples), "generateNoiseSamples");
+        check(msosm_sim_awgn(seed, numberOfSamples, isSNRMode ? 1 : 0, mean, variance, snr, samples),
+              "generateNoiseSamples");
+        return samples;
+    }
+    void deallocate()
+    {
+        if (samples)
+            msosm_host_free(samples, 0);
+        samples = nullptr;
+    }
+
+    unsigned long long seed = 0;
+
+private:
+    float mean, variance;
+    unsigned long numberOfSamples;
+    bool isSNRMode;
+    float snr = 0.f;
+    Complex *samples = nullptr;
+};
+
+// ---------------------------------------------------------------------------
+// simulated_pulsar/include/simulated_complex_signal.h:9-63 -- two deltas per
+// period dispersed at DM, tiled, optional AWGN and uint16 codec, generated on
+// the GPU (msosm_sim_two_spike).  The plot_abs methods (matplotlib) are not
+// provided.
+// ---------------------------------------------------------------------------
+
+class SimulatedComplexSignal {
+public:
+    SimulatedComplexSignal(float bw_, float dm_, float f0_, float period_, std::string mode = "complex")
+        : data_type(std::move(mode)), bw(bw_), fs(bw_), kdm(4.15e15f), dm(dm_), f0(f0_), period(period_)
+    {
+        msosm_sim_two_spike_info info;
+        check(msosm_sim_two_spike_shape(bw, dm, f0, period, &info), "SimulatedComplexSignal");
+        Np = info.Np;
+        Nd = info.Nd;
+        range = info.range;
+        check(msosm_prepare_min_order_msosm(Nd, &M_min), "SimulatedComplexSignal");
+        M = M_min;
+    }
+    SimulatedComplexSignal(const SimulatedComplexSignal &) = delete;
+    SimulatedComplexSignal &operator=(const SimulatedComplexSignal &) = delete;
+    ~SimulatedComplexSignal() { release(); }
+
+    void generate_pulsar_signal(unsigned long repeat = 1, bool add_noise = false, float SNR = 0, bool pinned = true)
+    {
+        release();
+        pinned_ = pinned;
+        signal_size = repeat * Np;
+        check(msosm_host_alloc(sizeof(Complex) * signal_size, pinned ? 1 : 0, (void **)&signal),
+              "generate_pulsar_signal");
+        if (data_type == "uint16")
+            check(msosm_host_alloc(sizeof(uint16_pair) * signal_size, pinned ? 1 : 0, (void **)&signal_u16),
+                  "generate_pulsar_signal");
+        check(msosm_sim_two_spike(bw, dm, f0, period, repeat, add_noise ? 1 : 0, SNR, seed, signal, signal_u16,
+                                  &signal_power),
+              "generate_pulsar_signal");
+    }
+
+    Complex *signal = nullptr;
+    uint16_pair *signal_u16 = nullptr;
+    std::string data_type;
+    unsigned long signal_size = 0;
+    unsigned long Np = 0;
+    unsigned long Nd = 0;
+    unsigned long M = 0;
+    unsigned long M_min = 0;
+    unsigned long range = 0;
+    // not in the reference's public fields
+    float signal_power = 0.f;  // dB, measured over one period
+    unsigned long long seed = 0;
+
+private:
+    void release()
+    {
+        if (signal)
+            msosm_host_free(signal, pinned_ ? 1 : 0);
+        if (signal_u16)
+            msosm_host_free(signal_u16, pinned_ ? 1 : 0);
+        signal = nullptr;
+        signal_u16 = nullptr;
+    }
+    float bw, fs, kdm, dm, f0, period;
+    bool pinned_ = true;
+};
+
 }  // namespace msosm_b200

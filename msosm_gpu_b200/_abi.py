@@ -26,6 +26,9 @@ FLAG_OSM = 0x1
 FLAG_NO_SERIES = 0x2
 FLAG_TENSOR_F16 = 0x4
 FLAG_TENSOR_BF16 = 0x8
+FLAG_DISPERSE = 0x10
+SIM_TAG_PULSAR = 0
+SIM_TAG_AWGN = 1
 DETECT_POWER = 0
 DETECT_AMPLITUDE = 1
 
@@ -62,13 +65,36 @@ class Timing(ctypes.Structure):
     ]
 
 
+class SimTwoSpikeInfo(ctypes.Structure):
+    _fields_ = [("Np", ctypes.c_ulong), ("Nd", ctypes.c_ulong), ("range", ctypes.c_ulong), ("order", ctypes.c_ulong)]
+
+
+class SimPulsarParams(ctypes.Structure):
+    _fields_ = [
+        ("bw", ctypes.c_float),
+        ("f0", ctypes.c_float),
+        ("dm", ctypes.c_float),
+        ("period", ctypes.c_double),
+        ("fwhm", ctypes.c_double),
+        ("centre", ctypes.c_double),
+        ("snr", ctypes.c_double),
+        ("seed", ctypes.c_ulonglong),
+    ]
+
+
+class SimPulsarInfo(ctypes.Structure):
+    _fields_ = [("chunk", ctypes.c_ulong), ("M", ctypes.c_ulong), ("Nd", ctypes.c_ulong),
+                ("next_sample", ctypes.c_ulonglong)]
+
+
 _lib = None
 
 
 def _declare(L: ctypes.CDLL) -> None:
     f32, ul, i32, u32, vp = ctypes.c_float, ctypes.c_ulong, ctypes.c_int, ctypes.c_uint, ctypes.c_void_p
     pul, pi, pvp = ctypes.POINTER(ul), ctypes.POINTER(i32), ctypes.POINTER(vp)
-    pull = ctypes.POINTER(ctypes.c_ulonglong)
+    ull = ctypes.c_ulonglong
+    pull = ctypes.POINTER(ull)
     sig = {
         "msosm_last_error": (ctypes.c_char_p, []),
         "msosm_version": (i32, []),
@@ -118,6 +144,16 @@ def _declare(L: ctypes.CDLL) -> None:
         "msosm_dada_get_header": (i32, [vp, vp]),
         "msosm_dada_read_count": (i32, [vp, ul, pul]),
         "msosm_dada_read": (i32, [vp, ul, vp, vp]),
+        "msosm_host_alloc": (i32, [ctypes.c_size_t, i32, pvp]),
+        "msosm_host_free": (i32, [vp, i32]),
+        "msosm_sim_normals": (i32, [ull, ull, ul, u32, vp, vp]),
+        "msosm_sim_awgn": (i32, [ull, ul, i32, f32, f32, f32, vp]),
+        "msosm_sim_two_spike_shape": (i32, [f32, f32, f32, f32, ctypes.POINTER(SimTwoSpikeInfo)]),
+        "msosm_sim_two_spike": (i32, [f32, f32, f32, f32, ul, i32, f32, ull, vp, vp, ctypes.POINTER(f32)]),
+        "msosm_sim_pulsar_create": (i32, [ctypes.POINTER(SimPulsarParams), ul, pvp]),
+        "msosm_sim_pulsar_destroy": (i32, [vp]),
+        "msosm_sim_pulsar_get_info": (i32, [vp, ctypes.POINTER(SimPulsarInfo)]),
+        "msosm_sim_pulsar_next": (i32, [vp, vp, vp, ctypes.c_double]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)

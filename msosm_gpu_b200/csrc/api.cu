@@ -268,80 +268,131 @@ cudaError_t plan_grid(msosm_dedisp *d)
     return cudaSuccess;
 }
 
-// H of every trial for N above one thread block, in the permuted [k1][k2]
-// order of the four-step spectra, scaled by `scale`:
-//   conj(h) -> FFT_M -> un-permute + conj (= the unnormalised inverse M-point
-//   DFT of h, the reference's h) -> zero pad to N -> FFT_N (permuted).
-msosm_status design_filters_large(int log2n, const std::vector<ChirpParams> &cp, float scale, float2 *Hp,
-                                  cudaStream_t st)
+}  // namespace
+
+// ---------------------------------------------------------------------------
+// Inverse M-point DFT of the reference chirp on the device (filter design and
+// the signal simulator)
+// ---------------------------------------------------------------------------
+
+namespace msosm {
+
+int ChirpIdft::init(int log2m_, cudaStream_t st)
 {
-    const long long N = 1ll << log2n, M = N / 2;
-    const int log2m = log2n - 1;
-    int n1l, n2l, m1l = 0, m2l = 0;
-    large_split(log2n, n1l, n2l);
-    const bool m_large = log2m > kMaxLog2N;
-    if (m_large)
-        large_split(log2m, m1l, m2l);
+    log2m = log2m_;
+    large = log2m > kMaxLog2N;
+    if (log2m < kMinLog2N || (large && !large_supported(log2m)))
+        return fail(MSOSM_ERR_UNSUPPORTED, "chirp transform of 2^%d points outside 2^%d .. 2^24", log2m, kMinLog2N);
+    const long long M = 1ll << log2m;
     size_t tot = 0;
-    ChirpParams *cp_d = nullptr;
-    float2 *V = nullptr, *W = nullptr, *P = nullptr, *A = nullptr;
-    float2 *twm1 = nullptr, *twm2 = nullptr, *twn1 = nullptr, *twn2 = nullptr;
-    msosm_status s = MSOSM_OK;
-    cudaError_t e = cudaMalloc((void **)&cp_d, sizeof(ChirpParams) * cp.size());
+    cudaError_t e = cudaMalloc((void **)&cp_d, sizeof(ChirpParams));
     if (e == cudaSuccess)
         e = dalloc(&V, (size_t)M, tot);
     if (e == cudaSuccess)
         e = dalloc(&W, (size_t)M, tot);
+    if (e == cudaSuccess && large)
+        e = dalloc(&A, (size_t)M, tot);
+    if (e != cudaSuccess) {
+        release();
+        return cuda_fail(e, "chirp transform scratch");
+    }
+    msosm_status s;
+    if (large) {
+        large_split(log2m, m1l, m2l);
+        s = upload_table(&tw1, 1 << m1l, -1, tot, st);
+        if (s == MSOSM_OK)
+            s = upload_table(&tw2, 1 << m2l, -1, tot, st);
+    } else {
+        s = upload_table(&tw1, 1 << log2m, -1, tot, st);
+    }
+    if (s != MSOSM_OK)
+        release();
+    return s;
+}
+
+// conj(chirp) -> FFT_M -> un-permute + conj: the unnormalised inverse DFT
+cudaError_t ChirpIdft::run(const ChirpParams &cp, int sign, float2 *P, long long len_out, cudaStream_t st)
+{
+    const long long M = 1ll << log2m;
+    cudaError_t e = cudaMemcpyAsync(cp_d, &cp, sizeof(ChirpParams), cudaMemcpyHostToDevice, st);
     if (e == cudaSuccess)
-        e = dalloc(&P, (size_t)N, tot);
-    if (e == cudaSuccess)
-        e = dalloc(&A, (size_t)N, tot);
+        e = launch_chirp_conj(cp_d, V, M, sign, st);
     if (e != cudaSuccess)
-        s = cuda_fail(e, "design scratch");
-    if (s == MSOSM_OK && m_large)
-        s = upload_table(&twm1, 1 << m1l, -1, tot, st);
-    if (s == MSOSM_OK && m_large)
-        s = upload_table(&twm2, 1 << m2l, -1, tot, st);
-    if (s == MSOSM_OK && !m_large)
-        s = upload_table(&twm1, 1 << log2m, -1, tot, st);
+        return e;
+    if (!large) {
+        e = launch_vec_fft(log2m, -1, V, W, tw1, 1, st);
+        if (e == cudaSuccess)
+            e = launch_unpermute_conj(W, P, M, 1, M, len_out, st);
+        return e;
+    }
+    LargeColArgs ca{};
+    ca.input = V;
+    ca.out = A;
+    ca.N = M;
+    ca.N2 = 1ll << m2l;
+    ca.len = M;
+    ca.log2n = log2m;
+    ca.count = 1;
+    ca.tw1 = tw1;
+    e = launch_large_col_fwd(m1l, 2, ca, 1, st);
+    if (e == cudaSuccess) {
+        LargeRowArgs ra{};
+        ra.in = A;
+        ra.out = W;
+        ra.N = M;
+        ra.log2n = log2m;
+        ra.tw2 = tw2;
+        ra.count = 1;
+        e = launch_large_row(m2l, 2, ra, 1 << m1l, 1, 1, st);
+    }
+    if (e == cudaSuccess)
+        e = launch_unpermute_conj(W, P, M, 1ll << m1l, 1ll << m2l, len_out, st);
+    return e;
+}
+
+void ChirpIdft::release()
+{
+    void *bufs[] = {cp_d, V, W, A, tw1, tw2};
+    for (void *b : bufs)
+        if (b)
+            cudaFree(b);
+    cp_d = nullptr;
+    V = W = A = tw1 = tw2 = nullptr;
+}
+
+}  // namespace msosm
+
+namespace {
+
+// H of every trial for N above one thread block, in the permuted [k1][k2]
+// order of the four-step spectra, scaled by `scale`:
+//   the unnormalised inverse M-point DFT of the chirp (the reference's h)
+//   -> zero pad to N -> FFT_N (permuted) -> x scale.
+msosm_status design_filters_large(int log2n, const std::vector<ChirpParams> &cp, float scale, int sign, float2 *Hp,
+                                  cudaStream_t st)
+{
+    const long long N = 1ll << log2n;
+    int n1l, n2l;
+    large_split(log2n, n1l, n2l);
+    size_t tot = 0;
+    ChirpIdft idft;
+    float2 *P = nullptr, *A = nullptr, *twn1 = nullptr, *twn2 = nullptr;
+    msosm_status s = idft.init(log2n - 1, st);
+    cudaError_t e = cudaSuccess;
+    if (s == MSOSM_OK) {
+        e = dalloc(&P, (size_t)N, tot);
+        if (e == cudaSuccess)
+            e = dalloc(&A, (size_t)N, tot);
+        if (e != cudaSuccess)
+            s = cuda_fail(e, "design scratch");
+    }
     if (s == MSOSM_OK)
         s = upload_table(&twn1, 1 << n1l, -1, tot, st);
     if (s == MSOSM_OK)
         s = upload_table(&twn2, 1 << n2l, -1, tot, st);
     if (s == MSOSM_OK) {
-        e = cudaMemcpyAsync(cp_d, cp.data(), sizeof(ChirpParams) * cp.size(), cudaMemcpyHostToDevice, st);
         for (size_t i = 0; i < cp.size() && e == cudaSuccess; ++i) {
-            e = launch_chirp_conj(cp_d + i, V, M, -1, st);
-            if (e != cudaSuccess)
-                break;
-            if (m_large) {
-                LargeColArgs ca{};
-                ca.input = V;
-                ca.out = A;
-                ca.N = M;
-                ca.N2 = 1ll << m2l;
-                ca.len = M;
-                ca.log2n = log2m;
-                ca.count = 1;
-                ca.tw1 = twm1;
-                e = launch_large_col_fwd(m1l, 2, ca, 1, st);
-                if (e == cudaSuccess) {
-                    LargeRowArgs ra{};
-                    ra.in = A;
-                    ra.out = W;
-                    ra.N = M;
-                    ra.log2n = log2m;
-                    ra.tw2 = twm2;
-                    ra.count = 1;
-                    e = launch_large_row(m2l, 2, ra, 1 << m1l, 1, 1, st);
-                }
-                if (e == cudaSuccess)
-                    e = launch_unpermute_conj(W, P, M, 1ll << m1l, 1ll << m2l, N, st);
-            } else {
-                e = launch_vec_fft(log2m, -1, V, W, twm1, 1, st);
-                if (e == cudaSuccess)
-                    e = launch_unpermute_conj(W, P, M, 1, M, N, st);
-            }
+            e = idft.run(cp[i], sign, P, N, st);
             if (e == cudaSuccess) {
                 LargeColArgs ca{};
                 ca.input = P;
@@ -372,7 +423,8 @@ msosm_status design_filters_large(int log2n, const std::vector<ChirpParams> &cp,
         if (e != cudaSuccess)
             s = cuda_fail(e, "large filter design");
     }
-    void *bufs[] = {cp_d, V, W, P, A, twm1, twm2, twn1, twn2};
+    idft.release();
+    void *bufs[] = {P, A, twn1, twn2};
     for (void *b : bufs)
         if (b)
             cudaFree(b);
@@ -485,8 +537,12 @@ msosm_status msosm_dedisp_create(const float *bw, const float *dm, const float *
     if (!out || !bw || !dm || !f0 || numDMs < 1)
         return fail(MSOSM_ERR_BAD_ARG, "msosm_dedisp_create: null argument or numDMs < 1");
     *out = nullptr;
-    if (flags & ~(MSOSM_FLAG_OSM | MSOSM_FLAG_NO_SERIES | MSOSM_FLAG_TENSOR_F16 | MSOSM_FLAG_TENSOR_BF16))
+    if (flags & ~(MSOSM_FLAG_OSM | MSOSM_FLAG_NO_SERIES | MSOSM_FLAG_TENSOR_F16 | MSOSM_FLAG_TENSOR_BF16 |
+                  MSOSM_FLAG_DISPERSE))
         return fail(MSOSM_ERR_BAD_ARG, "unknown flags 0x%x", flags);
+    // the per-bin block delays of MS-OSM follow the dedispersion chirp
+    if ((flags & MSOSM_FLAG_DISPERSE) && !(flags & MSOSM_FLAG_OSM))
+        return fail(MSOSM_ERR_BAD_ARG, "MSOSM_FLAG_DISPERSE needs MSOSM_FLAG_OSM");
     for (int i = 0; i < numDMs; ++i)
         if (!(bw[i] > 0) || !(f0[i] > 0) || !(dm[i] >= 0) || !std::isfinite(dm[i]))
             return fail(MSOSM_ERR_BAD_ARG, "trial %d: bw, f0 must be > 0 and dm >= 0", i);
@@ -633,6 +689,8 @@ msosm_status msosm_dedisp_create(const float *bw, const float *dm, const float *
         cp[i] = chirp_params(bw[i], dm[i], f0[i], M);
     // 1/N^2: the reference's /N before and /(2M) after the inverse FFT
     const float scale = 1.0f / ((float)N * (float)N);
+    // the dispersion filter (+phase chirp) of MSOSM_FLAG_DISPERSE
+    const int sign = (flags & MSOSM_FLAG_DISPERSE) ? +1 : -1;
     if (!d->large) {
         if ((s = upload_table(&d->tw_fwd, (int)N, -1, tot, d->stream)) != MSOSM_OK ||
             (s = upload_table(&d->tw_inv, (int)N, +1, tot, d->stream)) != MSOSM_OK ||
@@ -640,7 +698,7 @@ msosm_status msosm_dedisp_create(const float *bw, const float *dm, const float *
             release(d);
             return s;
         }
-        if ((s = design_filters(log2n, cp, scale, -1, d->tw_inv_m, d->tw_fwd, d->H, d->stream)) != MSOSM_OK) {
+        if ((s = design_filters(log2n, cp, scale, sign, d->tw_inv_m, d->tw_fwd, d->H, d->stream)) != MSOSM_OK) {
             release(d);
             return s;
         }
@@ -686,7 +744,7 @@ msosm_status msosm_dedisp_create(const float *bw, const float *dm, const float *
         }
         CKD(dalloc(&d->lA, (size_t)count * N, tot));
         CKD(dalloc(&d->lB, (size_t)numDMs * count * N, tot));
-        if ((s = design_filters_large(log2n, cp, scale, d->H, d->stream)) != MSOSM_OK) {
+        if ((s = design_filters_large(log2n, cp, scale, sign, d->H, d->stream)) != MSOSM_OK) {
             release(d);
             return s;
         }

@@ -174,4 +174,20 @@ cudaError_t launch_unpermute_conj(const float2 *in, float2 *out, long long K, lo
                                   long long len_out, cudaStream_t st);
 cudaError_t launch_conj_scale(float2 *x, long long n, float scale, int conj, cudaStream_t st);
 
+// Unnormalised inverse M-point DFT (M = 2^log2m, 64 .. 2^24) of the
+// reference chirp, sign -1 the dedispersion chirp (msosm_prepare.cpp:40-70)
+// and +1 the dispersion chirp of the signal simulator
+// (simulated_complex_signal.cpp:91-107), written to P[0, M) with zeros in
+// P[M, len_out).  init() allocates the scratch and twiddle tables (status
+// codes of msosm_b200.h); run() is ordered on its stream.
+struct ChirpIdft {
+    int log2m = 0, m1l = 0, m2l = 0;
+    bool large = false;
+    ChirpParams *cp_d = nullptr;
+    float2 *V = nullptr, *W = nullptr, *A = nullptr, *tw1 = nullptr, *tw2 = nullptr;
+    int init(int log2m, cudaStream_t st);
+    cudaError_t run(const ChirpParams &cp, int sign, float2 *P, long long len_out, cudaStream_t st);
+    void release();
+};
+
 }  // namespace msosm

@@ -17,6 +17,9 @@ from __future__ import annotations
 import argparse
 import ctypes
 import os
+import queue
+import threading
+import time
 from typing import Optional
 
 import numpy as np
@@ -112,15 +115,91 @@ def write_dada(path: str, pol1: np.ndarray, pol2: np.ndarray, bw_mhz: float = 16
         f.write(frames.tobytes())
 
 
+class _PinnedPairs:
+    """``n`` pairs of pinned host buffers of `samples` uint16 pairs."""
+
+    def __init__(self, n: int, samples: int):
+        self._ptrs = []
+        self.pairs = []
+        for _ in range(n):
+            pair = []
+            for _ in range(2):
+                p = ctypes.c_void_p()
+                check(lib().msosm_host_alloc(samples * 4, 1, ctypes.byref(p)))
+                self._ptrs.append(p)
+                buf = (ctypes.c_uint16 * (2 * samples)).from_address(p.value)
+                pair.append(np.ctypeslib.as_array(buf).reshape(samples, 2))
+            self.pairs.append(tuple(pair))
+
+    def close(self) -> None:
+        for p in self._ptrs:
+            lib().msosm_host_free(p, 1)
+        self._ptrs, self.pairs = [], []
+
+
+def _reads(f: PSRDADA, overlap: bool, depth: int = 3):
+    """Yields (pol1, pol2) of every whole read of the file in order.  With
+    ``overlap`` a reader thread fills `depth` pinned buffer pairs ahead of
+    the consumer (file I/O under the device work; a pair is handed back when
+    the consumer asks for the next one, after its filter calls have copied it
+    to the device)."""
+    n = f.pol1_in.shape[0]
+    if not overlap:
+        for _ in range(f.readCount):
+            f.readSamples()
+            yield f.pol1_in, f.pol2_in
+        return
+    bufs = _PinnedPairs(depth, n)
+    free: "queue.Queue" = queue.Queue()
+    ready: "queue.Queue" = queue.Queue()
+    for b in bufs.pairs:
+        free.put(b)
+    stop = threading.Event()
+
+    def reader():
+        try:
+            for _ in range(f.readCount):
+                b = free.get()
+                if stop.is_set():
+                    break
+                check(lib().msosm_dada_read(f._h, n, b[0].ctypes.data, b[1].ctypes.data))
+                ready.put(b)
+            ready.put(None)
+        except BaseException as e:  # handed to the consumer
+            ready.put(e)
+
+    t = threading.Thread(target=reader, daemon=True)
+    t.start()
+    try:
+        while True:
+            b = ready.get()
+            if b is None:
+                break
+            if isinstance(b, BaseException):
+                raise b
+            yield b
+            free.put(b)
+    finally:
+        stop.set()
+        free.put(None)
+        t.join()
+        bufs.close()
+
+
 def fold_file(filename: str, dm: float, period: float, fftpoint: int = 2097152, count: int = 1,
-              time_bin: int = 1024, precision: str = "fp32", write: bool = True) -> np.ndarray:
+              time_bin: int = 1024, precision: str = "fp32", write: bool = True, overlap: bool = True,
+              stats: Optional[dict] = None) -> np.ndarray:
     """The two-polarisation pipeline of msosm_psrdada.cpp:92-144 on a
     PSRDADA file; returns the folded profile (time_bin bins) and, with
     ``write``, writes it one value per line to the file's
-    ``*_dedisp_folded.txt`` (Fold_GPU::write_to_file)."""
+    ``*_dedisp_folded.txt`` (Fold_GPU::write_to_file).  ``overlap`` reads the
+    file on a second thread into pinned buffers while the device works (the
+    reads, their order and the result are the same either way); ``stats``
+    receives the samples processed and the wall time."""
     from .dedisp import Dedisperser
     from .fold import Fold_GPU
 
+    t0 = time.perf_counter()
     f = PSRDADA(filename)
     # band in MHz from the header, lower edge f0 = FREQ - BW/2, both in float
     bw = np.float32(f.bw)
@@ -134,18 +213,21 @@ def fold_file(filename: str, dm: float, period: float, fftpoint: int = 2097152, 
     fold = Fold_GPU(period, bw, count * M, time_bin=time_bin)
     fold.discard_samples(int(a.Nd[0]))
     first = True
-    for _ in range(f.readCount):
-        f.readSamples()
+    reads = 0
+    for p1, p2 in _reads(f, overlap):
+        reads += 1
         # blank data at the head of the file is skipped
         if first:
-            if f.pol1_in[0, 0] == 0:
+            if p1[0, 0] == 0:
                 continue
             first = False
-        a.filter_block(f.pol1_in)
-        b.filter_block(f.pol2_in)
+        a.filter_block(p1)
+        b.filter_block(p2)
         fold.calculate_intensity(a, b)
         fold.fold_data()
     prof = fold.fold_data_bins()
+    if stats is not None:
+        stats.update(samples=reads * count * M, seconds=time.perf_counter() - t0, reads=reads)
     if write:
         with open(f.outfileName, "w") as out:
             for v in prof:
@@ -163,10 +245,16 @@ def main() -> None:
     ap.add_argument("--period", type=float, required=True)
     ap.add_argument("--fftpoint", type=int, default=2097152)
     ap.add_argument("--time-bin", type=int, default=1024)
-    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp16"])
+    ap.add_argument("--count", type=int, default=1, help="FFT blocks per read")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp16", "bf16"])
+    ap.add_argument("--no-overlap", action="store_true", help="read the file on the calling thread")
     a = ap.parse_args()
-    prof = fold_file(a.file, a.dm, a.period, a.fftpoint, 1, a.time_bin, a.precision)
-    print(f"folded {prof.size} bins -> {os.path.splitext(a.file)[0]}_dedisp_folded.txt")
+    st = {}
+    prof = fold_file(a.file, a.dm, a.period, a.fftpoint, a.count, a.time_bin, a.precision,
+                     overlap=not a.no_overlap, stats=st)
+    print(f"folded {prof.size} bins -> {os.path.splitext(a.file)[0]}_dedisp_folded.txt; "
+          f"{st['samples']} samples per polarisation in {st['seconds']:.2f} s "
+          f"({st['samples'] / st['seconds'] / 1e6:.1f} Msamples/s)")
 
 
 if __name__ == "__main__":

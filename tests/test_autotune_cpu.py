@@ -1,0 +1,46 @@
+"""Host logic of the autotuner and of the uneven-batch workload (no GPU):
+candidate sets follow the MS-OSM minimum order and the error budget; fixed
+configurations are raised to an observation's minimum and fall back to FP32
+where the tensor path has no kernel; the workload's observations follow
+their stated distributions."""
+import numpy as np
+import pytest
+
+import bench
+from msosm_gpu_b200 import autotune as A
+from msosm_gpu_b200.prepare import msosm_min_order, nd
+
+
+def test_candidates_respect_minimum_and_budget():
+    dms = np.linspace(0, 100, 64).astype(np.float32)
+    m_min = max(msosm_min_order(nd(16e6, float(d), 1242e6)) for d in dms)
+    c = A.candidates(16e6, dms, 1242e6)
+    assert all(n >= 2 * m_min for n, _ in c)
+    assert (4096, "fp16") in c and (8192, "fp16") in c
+    assert not any(p == "bf16" for _, p in c)  # bf16 profiles exceed 1e-3
+    assert any(p == "bf16" for _, p in A.candidates(16e6, dms, 1242e6, budget=5e-3))
+    assert [p for _, p in A.candidates(16e6, dms, 1242e6, budget=1e-5)] == ["fp32"] * len(
+        {n for n, _ in c})
+    # a long smear leaves no tensor candidate
+    big = A.candidates(64e6, [300.0], 1068e6)
+    assert all(p == "fp32" and n >= 16384 for n, p in big)
+
+
+def test_fixed_choice():
+    assert A.fixed_choice(16e6, [50.0], 1242e6, 4096, "fp16") == (4096, "fp16")
+    n, p = A.fixed_choice(64e6, [300.0], 1068e6, 4096, "fp16")
+    assert n >= 16384 and p == "fp32"
+    assert A.fixed_choice(16e6, [1.0], 1242e6, 2048, "fp32") == (2048, "fp32")
+
+
+def test_uneven_observations():
+    obs = bench.uneven_observations(64, 0)
+    assert len(obs) == 64
+    n = np.array([o["n"] for o in obs])
+    assert n.min() >= 1 << 19 and n.max() <= 1 << 25 and np.all(n % (1 << 15) == 0)
+    assert {o["bw"] for o in obs} <= {4e6, 16e6, 32e6, 64e6}
+    for o in obs:
+        assert 1100e6 <= o["f0"] + o["bw"] / 2 <= 1500e6 + 1
+        assert 16 <= o["trials"] <= 512 and 20 <= o["dm_max"] <= 300
+        assert 0 < o["dm"] <= 0.9 * o["dm_max"] and 1e-3 <= o["period"] <= 1.0
+    assert obs == bench.uneven_observations(64, 0)

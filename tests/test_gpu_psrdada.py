@@ -59,6 +59,28 @@ def test_psrdada_two_pol_fold_matches_oracle(tmp_path, blank_reads):
     np.testing.assert_allclose(written, ours, rtol=1e-5)
     # the pulse is found at the injected phase: profile peak well above the median
     assert ours.max() > 1.5 * np.median(ours)
+    # reading on a second thread into pinned buffers changes nothing
+    st = {}
+    same = P.fold_file(path, dm, period, fftpoint=fftpoint, time_bin=tb, write=False, overlap=False, stats=st)
+    np.testing.assert_array_equal(same, ours)
+    assert st["reads"] == 40 and st["samples"] == 40 * 4096
+
+
+def test_psrdada_streaming_reads(tmp_path):
+    """Many reads with count > 1 (several FFT blocks per read): the
+    overlapped reader keeps order and covers the whole file."""
+    dm, period, fftpoint, tb, count = 8.0, 0.0021, 4096, 128, 4
+    bw, f0 = BW_MHZ * 1e6, (FREQ_MHZ - BW_MHZ / 2) * 1e6
+    n = 2048 * count * 25
+    a = S.quantise_uint16(S.pulsar_baseband(n, bw, f0, dm, period, 0.04, 2.0, seed=8), 300.0)
+    b = S.quantise_uint16(S.pulsar_baseband(n, bw, f0, dm, period, 0.04, 2.0, seed=9), 300.0)
+    path = str(tmp_path / "stream.dada")
+    P.write_dada(path, a, b, BW_MHZ, FREQ_MHZ)
+    st = {}
+    ov = P.fold_file(path, dm, period, fftpoint=fftpoint, count=count, time_bin=tb, write=False, stats=st)
+    sq = P.fold_file(path, dm, period, fftpoint=fftpoint, count=count, time_bin=tb, write=False, overlap=False)
+    np.testing.assert_array_equal(ov, sq)
+    assert st["reads"] == 25 and st["samples"] == n
 
 
 def test_psrdada_cpp_driver_matches_python_pipeline(tmp_path):
