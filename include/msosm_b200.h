@@ -336,6 +336,30 @@ MSOSM_API msosm_status msosm_dada_read(msosm_dada *d, unsigned long n, msosm_uin
                                        msosm_uint16_pair *pol2);
 
 /* ======================================================================
+ * Series files (the reference drivers' output writer threads)
+ * ====================================================================== */
+
+/* Appends every call's dedispersed series to a binary file while the device
+ * keeps working: the output-file threads of the reference's drivers
+ * (multiple_dm_concurrent_msosm.cpp:80-146), which write numDMs * count * M
+ * uint16 pairs per call, [dm][count*M], without the trailing element.
+ * msosm_writer_push (after a filter call, from the thread that drives the
+ * handle) encodes the call's series into one of `depth` device slots on the
+ * handle's stream -- the next call may start at once -- copies it to pinned
+ * host memory on the writer's own stream and queues it for the writer
+ * thread; it blocks only while all slots are in flight.  No busy-wait.
+ * kind: MSOSM_WRITE_UINT16 (the get_output_uint16 codec) or MSOSM_WRITE_C64.
+ * msosm_writer_close waits for the queued writes, closes the file and
+ * reports the bytes written (and the first error of the writer thread). */
+typedef struct msosm_writer msosm_writer;
+#define MSOSM_WRITE_UINT16 0
+#define MSOSM_WRITE_C64 1
+MSOSM_API msosm_status msosm_writer_create(msosm_dedisp *d, const char *path, int kind, int depth,
+                                           msosm_writer **out);
+MSOSM_API msosm_status msosm_writer_push(msosm_writer *w);
+MSOSM_API msosm_status msosm_writer_close(msosm_writer *w, unsigned long long *bytes_written);
+
+/* ======================================================================
  * Signal simulator (simulated_pulsar/) and host buffers
  * ====================================================================== */
 

@@ -24,6 +24,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <ctime>
 #include <cstdlib>
 #include <stdexcept>
 #include <string>
@@ -251,6 +252,7 @@ public:
     }
     void synchronize() { check(msosm_dedisp_synchronize(h_.h), "synchronize"); }
     void reset_device() { h_.reset(); }
+    msosm_dedisp *handle() const { return h_.h; }
 
     int count = 0;
     bool wait_for_cpu = false;
@@ -561,6 +563,48 @@ public:
 private:
     msosm_dada *h_ = nullptr;
     std::vector<uint16_pair> pol1_, pol2_;
+};
+
+// ---------------------------------------------------------------------------
+// Not a reference class: the output-file thread of the reference's drivers
+// (multiple_dm_concurrent_msosm.cpp:80-146: each call's numDMs * count * M
+// uint16 pairs appended to "<date time>_<numDMs>.bin") as an object over
+// msosm_writer_*.  push() after each filter call replaces get_output_thread
+// plus the wait_for_threads handshake; no busy-wait.
+// ---------------------------------------------------------------------------
+
+class SeriesFileWriter {
+public:
+    template <class Dedisperser>
+    SeriesFileWriter(Dedisperser &d, const std::string &path, int kind = MSOSM_WRITE_UINT16, int depth = 2)
+    {
+        check(msosm_writer_create(d.handle(), path.c_str(), kind, depth, &w_), "SeriesFileWriter");
+    }
+    SeriesFileWriter(const SeriesFileWriter &) = delete;
+    SeriesFileWriter &operator=(const SeriesFileWriter &) = delete;
+    ~SeriesFileWriter() { close(); }
+    void push() { check(msosm_writer_push(w_), "SeriesFileWriter::push"); }
+    unsigned long long close()
+    {
+        if (w_) {
+            msosm_writer *w = w_;
+            w_ = nullptr;
+            check(msosm_writer_close(w, &bytes_), "SeriesFileWriter::close");
+        }
+        return bytes_;
+    }
+    // the reference writer's file name: local date and time, the trial count
+    static std::string reference_name(int numDMs)
+    {
+        char buf[64];
+        std::time_t t = std::time(nullptr);
+        std::strftime(buf, sizeof buf, "%Y-%m-%d %H:%M:%S", std::localtime(&t));
+        return std::string(buf) + "_" + std::to_string(numDMs) + ".bin";
+    }
+
+private:
+    msosm_writer *w_ = nullptr;
+    unsigned long long bytes_ = 0;
 };
 
 // ---------------------------------------------------------------------------

@@ -27,6 +27,8 @@ FLAG_NO_SERIES = 0x2
 FLAG_TENSOR_F16 = 0x4
 FLAG_TENSOR_BF16 = 0x8
 FLAG_DISPERSE = 0x10
+WRITE_UINT16 = 0
+WRITE_C64 = 1
 SIM_TAG_PULSAR = 0
 SIM_TAG_AWGN = 1
 DETECT_POWER = 0
@@ -144,6 +146,9 @@ def _declare(L: ctypes.CDLL) -> None:
         "msosm_dada_get_header": (i32, [vp, vp]),
         "msosm_dada_read_count": (i32, [vp, ul, pul]),
         "msosm_dada_read": (i32, [vp, ul, vp, vp]),
+        "msosm_writer_create": (i32, [vp, ctypes.c_char_p, i32, i32, pvp]),
+        "msosm_writer_push": (i32, [vp]),
+        "msosm_writer_close": (i32, [vp, pull]),
         "msosm_host_alloc": (i32, [ctypes.c_size_t, i32, pvp]),
         "msosm_host_free": (i32, [vp, i32]),
         "msosm_sim_normals": (i32, [ull, ull, ul, u32, vp, vp]),

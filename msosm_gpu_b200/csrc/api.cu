@@ -431,6 +431,14 @@ msosm_status design_filters_large(int log2n, const std::vector<ChirpParams> &cp,
     return s;
 }
 
+}  // namespace
+
+namespace msosm {
+cudaStream_t dedisp_stream(const msosm_dedisp *d) { return d->stream; }
+}  // namespace msosm
+
+namespace {
+
 msosm_status check_handle(const msosm_dedisp *d)
 {
     if (!d)

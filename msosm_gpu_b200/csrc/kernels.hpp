@@ -5,6 +5,7 @@
 #include <cuda_runtime.h>
 
 #include "host_prepare.hpp"
+#include "msosm_b200.h"
 
 namespace msosm {
 
@@ -180,6 +181,10 @@ cudaError_t launch_conj_scale(float2 *x, long long n, float scale, int conj, cud
 // (simulated_complex_signal.cpp:91-107), written to P[0, M) with zeros in
 // P[M, len_out).  init() allocates the scratch and twiddle tables (status
 // codes of msosm_b200.h); run() is ordered on its stream.
+// The stream a dedispersion handle's work is ordered on (its own, or the one
+// set with msosm_dedisp_set_stream).
+cudaStream_t dedisp_stream(const msosm_dedisp *d);
+
 struct ChirpIdft {
     int log2m = 0, m1l = 0, m2l = 0;
     bool large = false;

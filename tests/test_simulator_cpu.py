@@ -102,3 +102,19 @@ def test_cpp_dropin_compiles(tmp_path):
                     str(tmp_path / "simulate_demo"), os.path.join(HERE, "cpp", "simulate_demo.cpp"),
                     "-L", os.path.join(root, "msosm_gpu_b200"), "-lmsosm_b200"], check=True, capture_output=True,
                    text=True)
+
+
+def test_writer_host_checks(tmp_path):
+    w = ctypes.c_void_p()
+    assert lib().msosm_writer_create(None, str(tmp_path / "x").encode(), 0, 2, ctypes.byref(w)) == _abi.ERR_BAD_ARG
+    assert lib().msosm_writer_close(None, None) == _abi.OK
+    subprocess_compile(tmp_path, "writer_demo")
+
+
+def subprocess_compile(tmp_path, name):
+    import subprocess
+    root = os.path.dirname(HERE)
+    subprocess.run(["g++", "-std=c++17", "-O2", "-Wall", "-I", os.path.join(root, "include"), "-o",
+                    str(tmp_path / name), os.path.join(HERE, "cpp", name + ".cpp"),
+                    "-L", os.path.join(root, "msosm_gpu_b200"), "-lmsosm_b200"], check=True, capture_output=True,
+                   text=True)
