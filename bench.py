@@ -798,7 +798,7 @@ def run_stream_to_file(args):
         for step in range(args.warmup + args.steps):
             fd, path = _tf.mkstemp(suffix=".bin", dir=tmpdir)
             os.close(fd)
-            w = SeriesWriter(d, path, kind="uint16", depth=2) if mode == "file" else None
+            w = SeriesWriter(d, path, kind="uint16", depth=4, threads=4) if mode == "file" else None
             torch.cuda.synchronize()
             t = time.perf_counter()
             for c in range(calls):

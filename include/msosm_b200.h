@@ -347,14 +347,16 @@ MSOSM_API msosm_status msosm_dada_read(msosm_dada *d, unsigned long n, msosm_uin
  * handle) encodes the call's series into one of `depth` device slots on the
  * handle's stream -- the next call may start at once -- copies it to pinned
  * host memory on the writer's own stream and queues it for the writer
- * thread; it blocks only while all slots are in flight.  No busy-wait.
+ * threads (1 .. depth); it blocks only while all slots are in flight.  No
+ * busy-wait.  Each batch lands at its own offset (call index x batch bytes),
+ * so several writer threads keep the file in call order.
  * kind: MSOSM_WRITE_UINT16 (the get_output_uint16 codec) or MSOSM_WRITE_C64.
  * msosm_writer_close waits for the queued writes, closes the file and
  * reports the bytes written (and the first error of the writer thread). */
 typedef struct msosm_writer msosm_writer;
 #define MSOSM_WRITE_UINT16 0
 #define MSOSM_WRITE_C64 1
-MSOSM_API msosm_status msosm_writer_create(msosm_dedisp *d, const char *path, int kind, int depth,
+MSOSM_API msosm_status msosm_writer_create(msosm_dedisp *d, const char *path, int kind, int depth, int threads,
                                            msosm_writer **out);
 MSOSM_API msosm_status msosm_writer_push(msosm_writer *w);
 MSOSM_API msosm_status msosm_writer_close(msosm_writer *w, unsigned long long *bytes_written);

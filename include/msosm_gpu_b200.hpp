@@ -576,9 +576,10 @@ private:
 class SeriesFileWriter {
 public:
     template <class Dedisperser>
-    SeriesFileWriter(Dedisperser &d, const std::string &path, int kind = MSOSM_WRITE_UINT16, int depth = 2)
+    SeriesFileWriter(Dedisperser &d, const std::string &path, int kind = MSOSM_WRITE_UINT16, int depth = 2,
+                     int threads = 1)
     {
-        check(msosm_writer_create(d.handle(), path.c_str(), kind, depth, &w_), "SeriesFileWriter");
+        check(msosm_writer_create(d.handle(), path.c_str(), kind, depth, threads, &w_), "SeriesFileWriter");
     }
     SeriesFileWriter(const SeriesFileWriter &) = delete;
     SeriesFileWriter &operator=(const SeriesFileWriter &) = delete;

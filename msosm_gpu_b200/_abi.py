@@ -146,7 +146,7 @@ def _declare(L: ctypes.CDLL) -> None:
         "msosm_dada_get_header": (i32, [vp, vp]),
         "msosm_dada_read_count": (i32, [vp, ul, pul]),
         "msosm_dada_read": (i32, [vp, ul, vp, vp]),
-        "msosm_writer_create": (i32, [vp, ctypes.c_char_p, i32, i32, pvp]),
+        "msosm_writer_create": (i32, [vp, ctypes.c_char_p, i32, i32, i32, pvp]),
         "msosm_writer_push": (i32, [vp]),
         "msosm_writer_close": (i32, [vp, pull]),
         "msosm_host_alloc": (i32, [ctypes.c_size_t, i32, pvp]),

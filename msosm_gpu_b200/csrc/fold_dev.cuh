@@ -127,39 +127,45 @@ __device__ __forceinline__ void fold_piece(const FoldArgs &f, float *prof, const
     }
 }
 
-// Fast path of fold_block: the block's M = 8 * blockDim.x samples all lie in
-// one span (phases ph_lo .. ph_lo + M - 1), bpt >= 8, so a thread's 8
-// samples touch at most two bins.  Samples whose bin is past the last output
-// bin are not folded (n_valid of them are).  Each thread sums its samples of
-// its first bin (and of the next one); every bin is then completed by the
-// thread holding its first sample (thread 0 for the bin running into the
-// block), adding the following threads' first-bin sums in thread order.
-template <bool PAD>
+// Fast path of fold_block: the SPT * blockDim.x samples all lie in one span
+// (phases ph_lo ..), bpt >= SPT, so a thread's SPT consecutive samples (8,
+// or 16 for a pair of blocks) touch at most two bins.  Samples whose bin is
+// past the last output bin are not folded (n_valid of them are).  Each
+// thread sums its samples of its first bin (and of the next one); every bin
+// is then completed by the thread holding its first sample (thread 0 for the
+// bin running into the range), adding the following threads' first-bin sums
+// in thread order.
+template <bool PAD, int SPT = 8>
 __device__ __forceinline__ void fold_block_fast(const FoldArgs &f, FoldSmem &w, float *prof, const float *ibuf,
                                                 int ph_lo, int n_valid)
 {
+    static_assert(SPT == 8 || (SPT == 16 && !PAD), "8 samples per thread, or 16 from a plain buffer");
     const int tid = threadIdx.x, T = blockDim.x;
     const int bpt = f.bpt;
-    const int j0 = 8 * tid;
+    const int j0 = SPT * tid;
     const int ph = ph_lo + j0;
     const int b0 = div_bpt(ph, bpt, f.inv_bpt);
     const int r0 = ph - b0 * bpt;  // place of the first sample in its bin
     const int n0 = bpt - r0;       // samples left in bin b0 (>= 1)
-    const int nv = min(8, n_valid - j0);
-    float x[8];
+    const int nv = min(SPT, n_valid - j0);
+    float x[SPT];
     if constexpr (PAD) {
 #pragma unroll
-        for (int u = 0; u < 8; ++u)
+        for (int u = 0; u < SPT; ++u)
             x[u] = ibuf[ipad(j0 + u)];
     } else {
-        const float4 lo = reinterpret_cast<const float4 *>(ibuf)[2 * tid];
-        const float4 hi = reinterpret_cast<const float4 *>(ibuf)[2 * tid + 1];
-        x[0] = lo.x; x[1] = lo.y; x[2] = lo.z; x[3] = lo.w;
-        x[4] = hi.x; x[5] = hi.y; x[6] = hi.z; x[7] = hi.w;
+#pragma unroll
+        for (int v = 0; v < SPT / 4; ++v) {
+            const float4 q = reinterpret_cast<const float4 *>(ibuf)[(SPT / 4) * tid + v];
+            x[4 * v] = q.x;
+            x[4 * v + 1] = q.y;
+            x[4 * v + 2] = q.z;
+            x[4 * v + 3] = q.w;
+        }
     }
     float s0 = 0.f, s1 = 0.f;
 #pragma unroll
-    for (int u = 0; u < 8; ++u) {
+    for (int u = 0; u < SPT; ++u) {
         const float v = u < nv ? x[u] : 0.f;
         if (u < n0)
             s0 += v;
@@ -174,7 +180,7 @@ __device__ __forceinline__ void fold_block_fast(const FoldArgs &f, FoldSmem &w, 
         // of the threads up to the bin's end
         auto finish = [&](int B, float acc) {
             const int e = min((B + 1) * bpt - ph_lo, n_valid);
-            for (int t = tid + 1; 8 * t < e; ++t)
+            for (int t = tid + 1; SPT * t < e; ++t)
                 acc += w.pa[t];
             prof[B] += acc;
         };
@@ -191,7 +197,7 @@ __device__ __forceinline__ void fold_block_fast(const FoldArgs &f, FoldSmem &w, 
     // long bins: G lanes per bin over the threads ta..tb that hold its samples
     // (first bin B when the thread's first phase is >= B*bpt, else its second)
     int g2 = 0;
-    while (g2 < 5 && (4 << g2) < (bpt >> 3) + 2)
+    while (g2 < 5 && (4 << g2) < bpt / SPT + 2)
         ++g2;
     const int G = 1 << g2, g = tid >> g2, l = tid & (G - 1), ngroups = T >> g2;
     const int b_first = div_bpt(ph_lo, bpt, f.inv_bpt);
@@ -201,16 +207,49 @@ __device__ __forceinline__ void fold_block_fast(const FoldArgs &f, FoldSmem &w, 
         float sum = 0.f;
         if (B <= b_last) {
             const int lo = B * bpt - ph_lo;
-            const int ta = lo > 0 ? (lo >> 3) : 0;
-            const int tb = min((B + 1) * bpt - 1 - ph_lo, n_valid - 1) >> 3;
+            const int ta = lo > 0 ? lo / SPT : 0;
+            const int tb = min((B + 1) * bpt - 1 - ph_lo, n_valid - 1) / SPT;
             for (int t = ta + l; t <= tb; t += G)
-                sum += (8 * t >= lo) ? w.pa[t] : w.pa[T + t];
+                sum += (SPT * t >= lo) ? w.pa[t] : w.pa[T + t];
         }
         for (int o = G >> 1; o > 0; o >>= 1)
             sum += __shfl_xor_sync(0xffffffffu, sum, o);
         if (B <= b_last && l == 0)
             prof[B] += sum;
     }
+}
+
+// Both blocks of a pair (2M contiguous intensities from chunk-local t0, M =
+// 8 * blockDim.x) in one pass of 16 samples per thread, when one span covers
+// them and bins hold >= 16 samples; false (nothing folded) when the caller
+// has to fold them block by block.
+__device__ __forceinline__ bool fold_pair(const FoldArgs &f, FoldSmem &w, const float *ibuf, int t0, int M, int &sp,
+                                          int &base, int &cnt)
+{
+    if (f.bpt < 16 || M != 8 * (int)blockDim.x)
+        return false;
+    while (sp < f.nspans) {
+        if (sp < base || sp >= base + cnt)
+            span_refill(f, w, sp, base, cnt);
+        if (w.wb[sp - base] <= t0)
+            ++sp;
+        else
+            break;
+    }
+    if (sp >= f.nspans)
+        return false;
+    const int i = sp - base;
+    const int sa = w.wa[i];
+    if (!(sa <= t0 && w.wb[i] >= t0 + 2 * M))
+        return false;
+    const int dest = w.wd[i];
+    if (dest != 0) {
+        const int ph_lo = w.wp[i] + (t0 - sa);
+        const int n_valid = min(2 * M, f.nbins * f.bpt - ph_lo);
+        if (n_valid > 0)
+            fold_block_fast<false, 16>(f, w, dest == 1 ? w.prof_main : w.prof_pend, ibuf, ph_lo, n_valid);
+    }
+    return true;
 }
 
 // Fold the M intensities of one block (ibuf: chunk-local samples t0..t0+M-1).

@@ -419,30 +419,32 @@ __global__ void __launch_bounds__(TcShape<LOG2N>::THREADS, TcShape<LOG2N>::CTAS_
             const long long kg = a.k0 + k;
             const int slot0 = (int)(kg & smask);
             if (kg >= a.max_delay && two) {
-                // every delayed block exists: no zero fill
+                // every delayed block exists: no zero fill.  No branch on the
+                // delays, so all 32 loads of the pair issue before the first
+                // use: each bin pair's first bin (with its neighbour, as one
+                // float4) from the first bin's row, the second bin again from
+                // its own row (the same L1 line when the delays agree)
+                float4 xa[8][2];
+                float2 xb[8][2];
 #pragma unroll
                 for (int j = 0; j < 8; ++j) {
                     const int q = (j * W + warp) * 32 + lane;  // float4 (bin pair) index in a row
-                    const float4 hv = hreg[j];
-                    const int d0 = (int)(dd[j] & 0xFFFFu), d1 = (int)(dd[j] >> 16);
-                    float4 x[2];
-                    if (d0 == d1) {
-                        const int r = (slot0 - d0) & smask;
-                        x[0] = ring4[(size_t)r * (N / 2) + q];
-                        x[1] = ring4[(size_t)((r + 1) & smask) * (N / 2) + q];
-                    } else {
-                        const int r0 = (slot0 - d0) & smask, r1 = (slot0 - d1) & smask;
-#pragma unroll
-                        for (int b = 0; b < 2; ++b) {
-                            const float2 t0 = ring2[(size_t)((r0 + b) & smask) * N + 2 * q];
-                            const float2 t1 = ring2[(size_t)((r1 + b) & smask) * N + 2 * q + 1];
-                            x[b] = make_float4(t0.x, t0.y, t1.x, t1.y);
-                        }
-                    }
+                    const int r0 = (slot0 - (int)(dd[j] & 0xFFFFu)) & smask;
+                    const int r1 = (slot0 - (int)(dd[j] >> 16)) & smask;
 #pragma unroll
                     for (int b = 0; b < 2; ++b) {
-                        const float zr0 = x[b].x * hv.x - x[b].y * hv.y, zi0 = x[b].x * hv.y + x[b].y * hv.x;
-                        const float zr1 = x[b].z * hv.z - x[b].w * hv.w, zi1 = x[b].z * hv.w + x[b].w * hv.z;
+                        xa[j][b] = ring4[(size_t)((r0 + b) & smask) * (N / 2) + q];
+                        xb[j][b] = ring2[(size_t)((r1 + b) & smask) * N + 2 * q + 1];
+                    }
+                }
+#pragma unroll
+                for (int j = 0; j < 8; ++j) {
+                    const float4 hv = hreg[j];
+#pragma unroll
+                    for (int b = 0; b < 2; ++b) {
+                        const float4 x = make_float4(xa[j][b].x, xa[j][b].y, xb[j][b].x, xb[j][b].y);
+                        const float zr0 = x.x * hv.x - x.y * hv.y, zi0 = x.x * hv.y + x.y * hv.x;
+                        const float zr1 = x.z * hv.z - x.w * hv.w, zi1 = x.z * hv.w + x.w * hv.z;
                         const int off = (b * 8 + j) * 128 + warp * 2048 + (lane >> 2) * 16 + (lane & 3) * 4;
                         *reinterpret_cast<uint32_t *>(op + off) = pack2<E>(zr0, zr1);
                         *reinterpret_cast<uint32_t *>(op + off + S::IM_OFF) = pack2<E>(zi0, zi1);
@@ -587,13 +589,17 @@ __global__ void __launch_bounds__(TcShape<LOG2N>::THREADS, TcShape<LOG2N>::CTAS_
                 outputs(i, sm + cur);
                 tc_fence_before();
                 if constexpr (FOLD) {
+                    // the pair's 2M intensities are contiguous: one pass when
+                    // one period span holds them, else block by block
                     const int k = kb + 2 * i;
                     const float *ib0 = reinterpret_cast<const float *>(sm + cur);
                     __syncthreads();
-                    fold_block<false>(a.fold, fw, ib0, k * M, M, sp, sbase, scnt);
-                    if (k + 1 < ke) {
-                        __syncthreads();
-                        fold_block<false>(a.fold, fw, ib0 + M, (k + 1) * M, M, sp, sbase, scnt);
+                    if (!(k + 1 < ke && fold_pair(a.fold, fw, ib0, k * M, M, sp, sbase, scnt))) {
+                        fold_block<false>(a.fold, fw, ib0, k * M, M, sp, sbase, scnt);
+                        if (k + 1 < ke) {
+                            __syncthreads();
+                            fold_block<false>(a.fold, fw, ib0 + M, (k + 1) * M, M, sp, sbase, scnt);
+                        }
                     }
                 }
                 if (more) {

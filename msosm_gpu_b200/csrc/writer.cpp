@@ -9,12 +9,14 @@
 // a free slot's device buffer on the handle's stream (so the next call's
 // kernels may overwrite the series at once), copies it to the slot's host
 // buffer on the writer's own copy stream (under the next call's compute) and
-// queues the slot; a writer thread waits on the copy's event, appends the
-// slot to the file and frees it.  Waits are on events and condition
-// variables; nothing spins.
+// queues the slot; one of `threads` writer threads waits on the copy's event,
+// writes the slot at its batch's offset in the file (pwrite: the file's
+// layout is the call order whatever thread writes a batch) and frees it.
+// Waits are on events and condition variables; nothing spins.
 #include "msosm_b200.h"
 
 #include <condition_variable>
+#include <cerrno>
 #include <cstdio>
 #include <deque>
 #include <mutex>
@@ -24,6 +26,8 @@
 #include <vector>
 
 #include <cuda_runtime.h>
+#include <fcntl.h>
+#include <unistd.h>
 
 #include "kernels.hpp"
 
@@ -50,9 +54,10 @@ struct msosm_writer {
     struct Slot {
         void *dev = nullptr, *host = nullptr;
         cudaEvent_t encoded = nullptr, copied = nullptr;
+        unsigned long long batch = 0;
     };
     msosm_dedisp *d = nullptr;
-    std::FILE *f = nullptr;
+    int fd = -1;
     int kind = MSOSM_WRITE_UINT16;
     size_t n = 0, elem = 0;  // elements (numDMs * count * M) and bytes per element
     cudaStream_t copy = nullptr;
@@ -60,11 +65,28 @@ struct msosm_writer {
     std::deque<int> free_q, write_q;
     std::mutex mu;
     std::condition_variable cv;
-    std::thread th;
+    std::vector<std::thread> th;
     bool closing = false;
     msosm_status err = MSOSM_OK;
     std::string errmsg;
-    unsigned long long bytes = 0, batches = 0;
+    unsigned long long bytes = 0, batches = 0, pushed = 0;
+
+    // all of buf at byte offset off
+    bool write_at(const void *buf, size_t len, unsigned long long off)
+    {
+        const char *p = static_cast<const char *>(buf);
+        while (len > 0) {
+            const ssize_t r = ::pwrite(fd, p, len, (off_t)off);
+            if (r < 0 && errno == EINTR)
+                continue;
+            if (r <= 0)
+                return false;
+            p += r;
+            len -= (size_t)r;
+            off += (unsigned long long)r;
+        }
+        return true;
+    }
 
     void run()
     {
@@ -79,14 +101,14 @@ struct msosm_writer {
                 write_q.pop_front();
             }
             cudaError_t e = cudaEventSynchronize(slots[s].copied);
-            size_t wrote = 0;
+            bool ok = false;
             if (e == cudaSuccess)
-                wrote = std::fwrite(slots[s].host, elem, n, f);
+                ok = write_at(slots[s].host, elem * n, slots[s].batch * (unsigned long long)(elem * n));
             std::lock_guard<std::mutex> lk(mu);
             if (e != cudaSuccess && err == MSOSM_OK) {
                 err = MSOSM_ERR_CUDA;
                 errmsg = std::string("writer copy: ") + cudaGetErrorString(e);
-            } else if (e == cudaSuccess && wrote != n && err == MSOSM_OK) {
+            } else if (e == cudaSuccess && !ok && err == MSOSM_OK) {
                 err = MSOSM_ERR_STATE;
                 errmsg = "writer: short write to the output file";
             } else if (e == cudaSuccess) {
@@ -114,15 +136,16 @@ struct msosm_writer {
         if (copy)
             cudaStreamDestroy(copy);
         copy = nullptr;
-        if (f)
-            std::fclose(f);
-        f = nullptr;
+        if (fd >= 0)
+            ::close(fd);
+        fd = -1;
     }
 };
 
 extern "C" {
 
-msosm_status msosm_writer_create(msosm_dedisp *d, const char *path, int kind, int depth, msosm_writer **out)
+msosm_status msosm_writer_create(msosm_dedisp *d, const char *path, int kind, int depth, int threads,
+                                 msosm_writer **out)
 {
     if (!d || !path || !out)
         return wfail(MSOSM_ERR_BAD_ARG, "msosm_writer_create: null argument");
@@ -131,6 +154,8 @@ msosm_status msosm_writer_create(msosm_dedisp *d, const char *path, int kind, in
         return wfail(MSOSM_ERR_BAD_ARG, "msosm_writer_create: kind must be MSOSM_WRITE_UINT16 or _C64");
     if (depth < 1 || depth > 16)
         return wfail(MSOSM_ERR_BAD_ARG, "msosm_writer_create: depth must be 1 .. 16");
+    if (threads < 1 || threads > depth)
+        return wfail(MSOSM_ERR_BAD_ARG, "msosm_writer_create: threads must be 1 .. depth");
     msosm_dedisp_info info;
     msosm_status st = msosm_dedisp_get_info(d, &info);
     if (st != MSOSM_OK)
@@ -144,8 +169,8 @@ msosm_status msosm_writer_create(msosm_dedisp *d, const char *path, int kind, in
     w->kind = kind;
     w->n = (size_t)info.numDMs * (size_t)info.count * info.M;
     w->elem = kind == MSOSM_WRITE_UINT16 ? sizeof(msosm_uint16_pair) : sizeof(msosm_complex);
-    w->f = std::fopen(path, "wb");
-    if (!w->f) {
+    w->fd = ::open(path, O_WRONLY | O_CREAT | O_TRUNC, 0644);
+    if (w->fd < 0) {
         delete w;
         return wfail(MSOSM_ERR_BAD_ARG, std::string("cannot open for writing: ") + path);
     }
@@ -167,7 +192,8 @@ msosm_status msosm_writer_create(msosm_dedisp *d, const char *path, int kind, in
         delete w;
         return wcuda(e, "msosm_writer_create");
     }
-    w->th = std::thread([w] { w->run(); });
+    for (int t = 0; t < threads; ++t)
+        w->th.emplace_back([w] { w->run(); });
     *out = w;
     return MSOSM_OK;
 }
@@ -186,6 +212,7 @@ msosm_status msosm_writer_push(msosm_writer *w)
         w->free_q.pop_front();
     }
     msosm_writer::Slot &sl = w->slots[s];
+    sl.batch = w->pushed;
     msosm_complex *series = nullptr;
     msosm_status st = msosm_dedisp_output_device_ptr(w->d, &series);
     cudaStream_t hs = dedisp_stream(w->d);
@@ -212,6 +239,7 @@ msosm_status msosm_writer_push(msosm_writer *w)
         return st != MSOSM_OK ? st : wcuda(e, "msosm_writer_push");
     }
     w->write_q.push_back(s);
+    w->pushed += 1;
     w->cv.notify_all();
     return MSOSM_OK;
 }
@@ -225,14 +253,11 @@ msosm_status msosm_writer_close(msosm_writer *w, unsigned long long *bytes_writt
         w->closing = true;
         w->cv.notify_all();
     }
-    if (w->th.joinable())
-        w->th.join();
+    for (std::thread &t : w->th)
+        if (t.joinable())
+            t.join();
     msosm_status st = w->err;
     std::string msg = w->errmsg;
-    if (st == MSOSM_OK && std::fflush(w->f) != 0) {
-        st = MSOSM_ERR_STATE;
-        msg = "writer: flush failed";
-    }
     if (bytes_written)
         *bytes_written = w->bytes;
     w->release();

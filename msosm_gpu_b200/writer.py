@@ -28,10 +28,11 @@ def reference_file_name(num_dms: int, thread_id=None) -> str:
 
 
 class SeriesWriter:
-    def __init__(self, dedisperser, path: str, kind: str = "uint16", depth: int = 2):
+    def __init__(self, dedisperser, path: str, kind: str = "uint16", depth: int = 2, threads: int = 1):
         k = {"uint16": _abi.WRITE_UINT16, "c64": _abi.WRITE_C64}[kind]
         h = ctypes.c_void_p()
-        check(lib().msosm_writer_create(dedisperser._h, path.encode(), k, int(depth), ctypes.byref(h)))
+        check(lib().msosm_writer_create(dedisperser._h, path.encode(), k, int(depth), int(threads),
+                                        ctypes.byref(h)))
         self._h = h
         self._d = dedisperser  # keeps the handle alive while the writer is open
         self.path = path

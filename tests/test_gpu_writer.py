@@ -17,14 +17,15 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 
 
-@pytest.mark.parametrize("kind,depth,precision", [("uint16", 2, "fp32"), ("c64", 3, "fp32"), ("uint16", 1, "fp16")])
-def test_writer_matches_get_output(tmp_path, kind, depth, precision):
+@pytest.mark.parametrize("kind,depth,threads,precision", [("uint16", 2, 1, "fp32"), ("c64", 3, 3, "fp32"),
+                                                          ("uint16", 1, 1, "fp16"), ("uint16", 4, 2, "fp16")])
+def test_writer_matches_get_output(tmp_path, kind, depth, threads, precision):
     dms, count, calls = [0.0, 3.0, 7.5], 6, 7
     d = Dedisperser(16e6, dms, 1242e6, 4096, count=count, precision=precision)
     x = G.pulsar_baseband(count * 2048 * calls, 16e6, 1242e6, 5.0, 0.002, 0.05, 1.0, seed=2)
     want = []
     path = str(tmp_path / f"series_{kind}.bin")
-    with SeriesWriter(d, path, kind=kind, depth=depth) as w:
+    with SeriesWriter(d, path, kind=kind, depth=depth, threads=threads) as w:
         for c in range(calls):
             d.filter_block(x[c * count * 2048:(c + 1) * count * 2048])
             w.push()

@@ -106,7 +106,7 @@ def test_cpp_dropin_compiles(tmp_path):
 
 def test_writer_host_checks(tmp_path):
     w = ctypes.c_void_p()
-    assert lib().msosm_writer_create(None, str(tmp_path / "x").encode(), 0, 2, ctypes.byref(w)) == _abi.ERR_BAD_ARG
+    assert lib().msosm_writer_create(None, str(tmp_path / "x").encode(), 0, 2, 1, ctypes.byref(w)) == _abi.ERR_BAD_ARG
     assert lib().msosm_writer_close(None, None) == _abi.OK
     subprocess_compile(tmp_path, "writer_demo")
 
