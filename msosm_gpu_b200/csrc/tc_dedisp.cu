@@ -420,10 +420,10 @@ __global__ void __launch_bounds__(TcShape<LOG2N>::THREADS, TcShape<LOG2N>::CTAS_
             const int slot0 = (int)(kg & smask);
             if (kg >= a.max_delay && two) {
                 // every delayed block exists: no zero fill.  No branch on the
-                // delays, so all 32 loads of the pair issue before the first
-                // use: each bin pair's first bin (with its neighbour, as one
-                // float4) from the first bin's row, the second bin again from
-                // its own row (the same L1 line when the delays agree)
+                // delays, so all loads of the pair issue before the first use:
+                // each bin pair as one float4 from the first bin's row, and,
+                // where the second bin's delay differs, that bin again from
+                // its own row (a predicated load)
                 float4 xa[8][2];
                 float2 xb[8][2];
 #pragma unroll
@@ -434,15 +434,18 @@ __global__ void __launch_bounds__(TcShape<LOG2N>::THREADS, TcShape<LOG2N>::CTAS_
 #pragma unroll
                     for (int b = 0; b < 2; ++b) {
                         xa[j][b] = ring4[(size_t)((r0 + b) & smask) * (N / 2) + q];
-                        xb[j][b] = ring2[(size_t)((r1 + b) & smask) * N + 2 * q + 1];
+                        xb[j][b] = r1 != r0 ? ring2[(size_t)((r1 + b) & smask) * N + 2 * q + 1]
+                                            : make_float2(0.f, 0.f);
                     }
                 }
 #pragma unroll
                 for (int j = 0; j < 8; ++j) {
                     const float4 hv = hreg[j];
+                    const bool split = (dd[j] & 0xFFFFu) != (dd[j] >> 16);
 #pragma unroll
                     for (int b = 0; b < 2; ++b) {
-                        const float4 x = make_float4(xa[j][b].x, xa[j][b].y, xb[j][b].x, xb[j][b].y);
+                        const float4 x = split ? make_float4(xa[j][b].x, xa[j][b].y, xb[j][b].x, xb[j][b].y)
+                                               : xa[j][b];
                         const float zr0 = x.x * hv.x - x.y * hv.y, zi0 = x.x * hv.y + x.y * hv.x;
                         const float zr1 = x.z * hv.z - x.w * hv.w, zi1 = x.z * hv.w + x.w * hv.z;
                         const int off = (b * 8 + j) * 128 + warp * 2048 + (lane >> 2) * 16 + (lane & 3) * 4;
