@@ -451,6 +451,47 @@ MSOSM_API msosm_status msosm_sim_pulsar_next(msosm_sim *s, msosm_complex *out, m
                                              double u16_scale);
 
 /* ======================================================================
+ * DM-proposal network (no counterpart in the reference)
+ * ====================================================================== */
+
+/* A small 1-D CNN over the folded profiles of in_channels coarse DM trials
+ * (length phase bins): `layers` circular convolutions of `channels` outputs
+ * and odd `kernel`, each with ReLU, the mean over phase, and two linear
+ * heads -- a detection logit and a DM offset.  Weights are kept in FP32 and
+ * used rounded to bf16; products accumulate in FP32; every reduction has a
+ * fixed order.  Loss: logistic loss of the logit plus dm_weight times the
+ * mean over positive samples of the squared offset error.  Parameters, one
+ * FP32 vector: per layer weights [C_out][C_in][kernel] then biases [C_out];
+ * detection head weights [channels] and bias; offset head weights and bias.
+ * in_channels and channels: multiples of 8; length: a multiple of 32. */
+typedef struct msosm_cnn msosm_cnn;
+typedef struct msosm_cnn_config {
+    int in_channels;  /* coarse DM trials per sample */
+    int length;       /* phase bins */
+    int channels;     /* convolution outputs */
+    int kernel;       /* odd kernel width */
+    int layers;
+    int max_batch;    /* <= 1024 */
+    float dm_weight;  /* weight of the offset loss */
+} msosm_cnn_config;
+/* He-uniform weights from `seed`, zero biases.  Needs a GPU. */
+MSOSM_API msosm_status msosm_cnn_create(const msosm_cnn_config *cfg, unsigned long long seed, msosm_cnn **out);
+MSOSM_API msosm_status msosm_cnn_destroy(msosm_cnn *n);
+MSOSM_API msosm_status msosm_cnn_param_count(const msosm_cnn *n, size_t *count);
+MSOSM_API msosm_status msosm_cnn_get_params(msosm_cnn *n, float *params);
+/* Also clears the optimiser's state. */
+MSOSM_API msosm_status msosm_cnn_set_params(msosm_cnn *n, const float *params);
+/* x: [batch][in_channels][length]; logit, offset: [batch]; host or device. */
+MSOSM_API msosm_status msosm_cnn_forward(msosm_cnn *n, const float *x, int batch, float *logit, float *offset);
+/* Loss and gradient of a batch (label 1 pulsar / 0 noise, target the offset
+ * of positive samples); the gradient stays for msosm_cnn_adam_step and is
+ * copied to `grad` (param_count floats) when it is not NULL. */
+MSOSM_API msosm_status msosm_cnn_gradient(msosm_cnn *n, const float *x, const float *label, const float *target,
+                                          int batch, float *loss, float *grad);
+/* One Adam step (beta 0.9, 0.999, eps 1e-8) with the last gradient. */
+MSOSM_API msosm_status msosm_cnn_adam_step(msosm_cnn *n, float lr);
+
+/* ======================================================================
  * Diagnostics (no counterpart in the reference)
  * ====================================================================== */
 

@@ -89,6 +89,12 @@ class SimPulsarInfo(ctypes.Structure):
                 ("next_sample", ctypes.c_ulonglong)]
 
 
+class CnnConfig(ctypes.Structure):
+    _fields_ = [("in_channels", ctypes.c_int), ("length", ctypes.c_int), ("channels", ctypes.c_int),
+                ("kernel", ctypes.c_int), ("layers", ctypes.c_int), ("max_batch", ctypes.c_int),
+                ("dm_weight", ctypes.c_float)]
+
+
 _lib = None
 
 
@@ -149,6 +155,14 @@ def _declare(L: ctypes.CDLL) -> None:
         "msosm_writer_create": (i32, [vp, ctypes.c_char_p, i32, i32, i32, pvp]),
         "msosm_writer_push": (i32, [vp]),
         "msosm_writer_close": (i32, [vp, pull]),
+        "msosm_cnn_create": (i32, [ctypes.POINTER(CnnConfig), ull, pvp]),
+        "msosm_cnn_destroy": (i32, [vp]),
+        "msosm_cnn_param_count": (i32, [vp, ctypes.POINTER(ctypes.c_size_t)]),
+        "msosm_cnn_get_params": (i32, [vp, vp]),
+        "msosm_cnn_set_params": (i32, [vp, vp]),
+        "msosm_cnn_forward": (i32, [vp, vp, i32, vp, vp]),
+        "msosm_cnn_gradient": (i32, [vp, vp, vp, vp, i32, ctypes.POINTER(f32), vp]),
+        "msosm_cnn_adam_step": (i32, [vp, f32]),
         "msosm_host_alloc": (i32, [ctypes.c_size_t, i32, pvp]),
         "msosm_host_free": (i32, [vp, i32]),
         "msosm_sim_normals": (i32, [ull, ull, ul, u32, vp, vp]),
