@@ -834,6 +834,103 @@ def run_stream_to_file(args):
 
 
 # ---------------------------------------------------------------------------
+# learned DM proposal: train on simulated pulsars, judge with the full sweep
+# ---------------------------------------------------------------------------
+
+def run_dm_proposal(args):
+    """Config 5 at reduced scale: a 32 MHz band at 1400 MHz, 2^24 samples per
+    observation, DM 0-500, period log-uniform 1 ms - 1 s, duty cycle 1-10 %,
+    peak SNR 0.01-0.2, half the observations noise only; 64 coarse trials
+    folded to 256 bins feed the network.  Held-out observations (again half
+    noise) are searched: the exhaustive fine sweep (4096 trials over 0-500)
+    judges every pulsar; the method without the network searches fine trials
+    in a window around the coarse trial of highest S/N in every observation;
+    with the network, only observations it flags (logit > 0) are searched,
+    around the coarse peak moved by the predicted offset.  A pulsar counts as
+    found when the window recovers >= 90 % of the sweep's best S/N."""
+    import torch
+    from msosm_gpu_b200 import dm_proposal as P
+    from msosm_gpu_b200.simulator import pulsar_baseband
+    band = P.Band()
+    t = time.time()
+    X, lab, tgt, meta = P.simulate_profiles(args.train, band, seed=1)
+    gen_s = time.time() - t
+    log(f"training set: {args.train} samples in {gen_s:.1f} s")
+    net = P.DMProposalNet(band.coarse, band.nbins, 32, 7, 4, max_batch=256, dm_weight=0.25, seed=0)
+    t = time.time()
+    hist = P.train(net, X, lab, tgt, epochs=args.epochs, batch=256, lr=2e-3, log=log)
+    train_s = time.time() - t
+    fine_step = band.dm_max / 4095
+    cs = band.dm_max / (band.coarse - 1)
+    windows = {"base2": 2.0, "net2": 2.0, "net1": 1.0}  # half widths in coarse steps
+    rng = np.random.default_rng(7)
+    rows = []
+    for i in range(args.eval):
+        p = P.draw_pulsar(rng, band)
+        pulsar = rng.random() >= 0.5
+        x = pulsar_baseband(band.samples, band.bw, band.f0, p["dm"], p["period"], p["duty"],
+                            p["snr"] if pulsar else 0.0, seed=1000 + i, device=torch.device("cuda"))
+        prof = P.fold_trials(x, band, band.coarse_dms, p["period"])
+        xin = P.normalise(prof)[None]
+        lg, of = net.forward(np.ascontiguousarray(xin))
+        k = P.coarse_peak(prof, p["duty"])
+        centres = {"base2": k * cs, "net2": (k + float(of[0])) * cs, "net1": (k + float(of[0])) * cs}
+        r = dict(p, pulsar=bool(pulsar), logit=float(lg[0]), offset=float(of[0]), coarse_peak=k * cs)
+        for name, hw in windows.items():
+            lo, hi = max(0.0, centres[name] - hw * cs), min(band.dm_max, centres[name] + hw * cs)
+            r[name + "_trials"] = int(np.floor((hi - lo) / fine_step)) + 1
+        if pulsar:
+            dms, snr = P.fine_search(x, band, p["period"], p["duty"], 0.0, band.dm_max, fine_step)
+            r["sweep_snr"], r["sweep_dm"] = float(snr.max()), float(dms[int(np.argmax(snr))])
+            for name, hw in windows.items():
+                wd, ws = P.fine_search(x, band, p["period"], p["duty"], centres[name] - hw * cs,
+                                       centres[name] + hw * cs, fine_step)
+                r[name + "_snr"] = float(ws.max()) if ws.size else 0.0
+                r[name + "_found"] = bool(r[name + "_snr"] >= 0.9 * r["sweep_snr"])
+        rows.append(r)
+        del x
+        log(f"eval {i}: pulsar {pulsar} dm {p['dm']:.1f} logit {lg[0]:.2f} offset {of[0]:.2f} "
+            + (f"sweep {r['sweep_dm']:.1f} snr {r['sweep_snr']:.1f} found base {r['base2_found']} "
+               f"net2 {r['net2_found']} net1 {r['net1_found']}" if pulsar else ""))
+    det = [r for r in rows if r["pulsar"] and r["sweep_snr"] >= args.snr_min]
+    flagged = lambda r: r["logit"] > 0  # noqa: E731
+
+    def recall(name, gate):
+        if not det:
+            return None
+        return sum(1 for r in det if r[name + "_found"] and (not gate or flagged(r))) / len(det)
+
+    def trials(name, gate):
+        return band.coarse + float(np.mean([r[name + "_trials"] if (not gate or flagged(r)) else 0
+                                            for r in rows]))
+
+    res = {"without_network_2steps": {"recall": recall("base2", False), "trials": trials("base2", False)},
+           "network_2steps": {"recall": recall("net2", True), "trials": trials("net2", True)},
+           "network_1step": {"recall": recall("net1", True), "trials": trials("net1", True)}}
+    for v in res.values():
+        v["reduction_vs_exhaustive"] = 4096.0 / v["trials"]
+    noise = [r for r in rows if not r["pulsar"]]
+    line = {"workload": "learned DM proposal (reduced scale): 32 MHz at 1400 MHz, 2^24 samples per observation, "
+                        "DM 0-500, period 1 ms-1 s, duty 1-10 %, peak SNR 0.01-0.2, half noise only; 64 coarse "
+                        "trials x 256 bins",
+            "network": "4 circular conv1d layers (32 channels, kernel 7, ReLU), mean over phase, detection and "
+                       "DM-offset heads; bf16 weights, FP32 accumulation; msosm_cnn_* kernels, Adam",
+            "train_samples": args.train, "noise_fraction": 0.5, "epochs": args.epochs,
+            "training_set_seconds": gen_s, "training_seconds": train_s,
+            "loss_first_last": [hist[0], hist[-1]] if hist else None,
+            "eval_observations": len(rows), "eval_pulsars": sum(1 for r in rows if r["pulsar"]),
+            "pulsars_detected_by_sweep": len(det), "snr_min": args.snr_min,
+            "noise_flagged": (sum(1 for r in noise if flagged(r)) / len(noise)) if noise else None,
+            "results": res, "exhaustive_trials": 4096,
+            "rule": "a pulsar is found when its fine window recovers >= 90 % of the exhaustive sweep's best S/N; "
+                    "recall over the pulsars the sweep detects (S/N >= snr_min); trials per observation include "
+                    "the 64 coarse ones",
+            "rows": rows}
+    print(json.dumps(line), flush=True)
+    net.close()
+
+
+# ---------------------------------------------------------------------------
 # reference arms
 # ---------------------------------------------------------------------------
 
@@ -915,11 +1012,16 @@ def main():
     ap.add_argument("--precision", default="fp16", choices=["fp32", "fp16", "bf16"],
                     help="inverse transforms on the CUDA cores (fp32) or the tensor cores (fp16, bf16)")
     ap.add_argument("--workload", default="batched",
-                    choices=["batched", "precision-sweep", "uneven-batch", "stream-to-file"],
+                    choices=["batched", "precision-sweep", "uneven-batch", "stream-to-file", "dm-proposal"],
                     help="batched: the 256-trial 16 MHz workload (the bench line); precision-sweep: the "
                          "64 MHz / FFT 8192 / 1024-trial sweep of the inverse-transform precisions; "
                          "uneven-batch: 64 independent observations, autotuned vs fixed configurations; "
-                         "stream-to-file: host input in, every trial's uint16 series written to a file")
+                         "stream-to-file: host input in, every trial's uint16 series written to a file; "
+                         "dm-proposal: the learned coarse-DM proposal against the exhaustive fine sweep")
+    ap.add_argument("--train", type=int, default=2048, help="dm-proposal: training samples")
+    ap.add_argument("--epochs", type=int, default=40, help="dm-proposal: training epochs")
+    ap.add_argument("--eval", type=int, default=96, help="dm-proposal: held-out observations (half noise)")
+    ap.add_argument("--snr-min", type=float, default=8.0, help="dm-proposal: sweep detection threshold")
     ap.add_argument("--obs", type=int, default=UNEVEN["n_obs"], help="uneven-batch: observations")
     ap.add_argument("--seeds", type=int, default=SWEEP["seeds"], help="precision-sweep: signal seeds")
     args = ap.parse_args()
@@ -929,7 +1031,7 @@ def main():
                               "reference arm"}))
             return
         {"precision-sweep": run_precision_sweep, "uneven-batch": run_uneven_batch,
-         "stream-to-file": run_stream_to_file}[args.workload](args)
+         "stream-to-file": run_stream_to_file, "dm-proposal": run_dm_proposal}[args.workload](args)
         return
     args.log2_samples = args.log2_samples or LOG2_SAMPLES
     args.dms = args.dms or N_DM
