@@ -420,6 +420,23 @@ def run_ours(args):
     else:
         roofline = dict(fp32_roofline(tm), traffic=traffic_of("bytes_per_dm_sample"))
         roofline_fp32 = None
+    # issue roofline of the tensor-core kernel: its warp instructions per
+    # DM-trial sample (ncu capture) at the measured rate, against 4 issue
+    # slots per SM per clock at the SM clock sampled during the run
+    roofline_issue = None
+    ipd = tr.get("tc_warp_inst_per_dm_sample")
+    if args.precision != "fp32" and ipd:
+        import torch as _t
+        sms = _t.cuda.get_device_properties(dev).multi_processor_count
+        mhz = (clocks or {}).get("sm_mhz") or (clocks or {}).get("sm_max_mhz") or 1965.0
+        k_ms = tm["dedisp_ms"] / max(tm["calls"], 1)
+        ach = ipd * launch_samples / (k_ms * 1e-3)
+        pk = 4.0 * sms * mhz * 1e6
+        roofline_issue = {"bound": "issue", "achieved": ach, "peak": pk, "unit": "warp instructions/s",
+                          "frac": ach / pk, "warp_inst_per_dm_sample": ipd,
+                          "note": "the tensor-core kernel is bound by CUDA-core issue (gather, twiddle, fold "
+                                  "and their barriers), not by HBM or the tensor pipe; instructions per sample "
+                                  "from profiles/roofline_traffic.json"}
     hbm = peaks.get("hbm_gbs")
     algo_bytes = 8.0 * samples  # the input, read once for all trials
     roofline_hbm = {"bound": "hbm", "algorithmic_bytes_per_step": algo_bytes,
@@ -445,6 +462,8 @@ def run_ours(args):
             "check": {"detected_dm": peak_dm, "injected_dm": PULSAR["dm"]}}
     if roofline_fp32:
         line["roofline_fp32_path"] = roofline_fp32
+    if roofline_issue:
+        line["roofline_issue"] = roofline_issue
     if rank == 0 and ws == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(dms, x)
         line["accuracy_vs_fp64"] = accuracy_vs_fp64(dms, x)
