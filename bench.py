@@ -349,7 +349,7 @@ def run_ours(args):
     value_other = units / (ms_o * 1e-3) / 1e6
 
     # ---- e2e: pinned host input through the C ABI, chunked calls -----------
-    e_count = min(blocks, 4096)
+    e_count = min(blocks, 8192)
     calls = blocks // e_count
     de = Dedisperser(BW, dms, F0, FFTPOINT, count=e_count, series=False, precision=args.precision)
     de.fold_init(PULSAR["period"], BW, time_bin=NBINS, discard_Nd=nd_max, detect="power")
