@@ -857,10 +857,11 @@ static msosm_status fold_prepare(msosm_dedisp *d, int sb, FoldArgs &fa)
         hp[i] = d->spans[i].phase0;
         hp[d->span_cap + i] = d->spans[i].dest;
     }
-    CK(cudaMemcpyAsync(d->span_a_d, h, sizeof(long long) * n, cudaMemcpyHostToDevice, d->stream));
-    CK(cudaMemcpyAsync(d->span_b_d, h + d->span_cap, sizeof(long long) * n, cudaMemcpyHostToDevice, d->stream));
-    CK(cudaMemcpyAsync(d->span_p_d, hp, sizeof(int) * n, cudaMemcpyHostToDevice, d->stream));
-    CK(cudaMemcpyAsync(d->span_dest_d, hp + d->span_cap, sizeof(int) * n, cudaMemcpyHostToDevice, d->stream));
+    // a kernel reads the staging: copies on this stream would wait behind the
+    // next call's input copy on the copy engine, and the dedispersion kernel
+    // with them
+    CK(launch_span_upload(h, n, d->span_cap, d->span_a_d, d->span_b_d, d->span_p_d, d->span_dest_d, d->stream));
+    d->launches += n > 0 ? 1 : 0;
     CK(cudaEventRecord(d->ev_spans[sb], d->stream));
     if (flush) {
         CK(launch_fold_flush(d->acc_main, d->acc_pend, (size_t)d->D * d->nbins, d->stream));

@@ -574,6 +574,35 @@ cudaError_t launch_fold_flush(double *am, double *ap, size_t n, cudaStream_t st)
     return cudaGetLastError();
 }
 
+// Reads pinned host memory directly (mapped, unified addressing), so the
+// upload is ordered on the compute stream alone and never waits behind a
+// large input copy on the copy engines
+__global__ void span_upload_kernel(const long long *__restrict__ h, int n, int cap, long long *__restrict__ a,
+                                   long long *__restrict__ b, int *__restrict__ p, int *__restrict__ dest)
+{
+    const int *hp = reinterpret_cast<const int *>(h + 2 * (size_t)cap);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        a[i] = h[i];
+        b[i] = h[cap + i];
+        p[i] = hp[i];
+        dest[i] = hp[cap + i];
+    }
+}
+
+cudaError_t launch_span_upload(const long long *host, int n, int cap, long long *a, long long *b, int *phase0,
+                               int *dest, cudaStream_t st)
+{
+    if (n <= 0)
+        return cudaSuccess;
+    void *hd = nullptr;
+    cudaError_t e = cudaHostGetDevicePointer(&hd, const_cast<long long *>(host), 0);
+    if (e != cudaSuccess)
+        return e;
+    const unsigned int g = blocks_for((size_t)n, 256) < 64 ? blocks_for((size_t)n, 256) : 64;
+    span_upload_kernel<<<g, 256, 0, st>>>(static_cast<const long long *>(hd), n, cap, a, b, phase0, dest);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_fold_readout(const double *am, size_t n, double scale, float *out, cudaStream_t st)
 {
     fold_readout_kernel<<<blocks_for(n, 256), 256, 0, st>>>(am, n, scale, out);

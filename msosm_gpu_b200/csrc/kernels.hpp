@@ -106,6 +106,11 @@ cudaError_t launch_design(int log2n, const DesignArgs &a, cudaStream_t st);
 cudaError_t launch_fold_reduce(const float *part_main, const float *part_pend, int D, int R, int nbins,
                                double *acc_main, double *acc_pend, cudaStream_t st);
 cudaError_t launch_fold_flush(double *acc_main, double *acc_pend, size_t n, cudaStream_t st);
+// The n fold spans of a call from their pinned host staging (a, b: long long
+// [cap] each, then phase0, dest: int [cap] each), read by a kernel over the
+// bus, into the device span arrays
+cudaError_t launch_span_upload(const long long *host, int n, int cap, long long *a, long long *b, int *phase0,
+                               int *dest, cudaStream_t st);
 cudaError_t launch_fold_readout(const double *acc_main, size_t n, double scale, float *out,
                                 cudaStream_t st);
 cudaError_t launch_encode_u16(const float2 *src, uint32_t *dst, size_t n, cudaStream_t st);
