@@ -1495,10 +1495,8 @@ msosm_status msosm_fold_data(msosm_fold *f)
         hp[i] = f->spans[i].phase0;
         hp[f->span_cap + i] = f->spans[i].dest;
     }
-    CK(cudaMemcpyAsync(f->span_a, h, sizeof(long long) * n, cudaMemcpyHostToDevice, f->stream));
-    CK(cudaMemcpyAsync(f->span_b, h + f->span_cap, sizeof(long long) * n, cudaMemcpyHostToDevice, f->stream));
-    CK(cudaMemcpyAsync(f->span_p, hp, sizeof(int) * n, cudaMemcpyHostToDevice, f->stream));
-    CK(cudaMemcpyAsync(f->span_dest, hp + f->span_cap, sizeof(int) * n, cudaMemcpyHostToDevice, f->stream));
+    // read by a kernel, not copied: see fold_prepare
+    CK(launch_span_upload(h, n, f->span_cap, f->span_a, f->span_b, f->span_p, f->span_dest, f->stream));
     if (flush)
         CK(launch_fold_flush(f->acc_main, f->acc_pend, (size_t)f->nbins, f->stream));
     CK(cudaMemsetAsync(f->part_main, 0, sizeof(float) * f->R * f->nbins, f->stream));
