@@ -81,3 +81,27 @@ def test_two_pol_pipeline_matches_reference_gpu_and_oracle():
         assert r.returncode == 0, r.stderr
         ref = O.read_records(fo)["folded"]
     assert rel_rms(ours, ref) < 1e-4, rel_rms(ours, ref)
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp16"])
+def test_fused_fold_with_many_spans_per_call(precision):
+    # a 10 us period at 16 MHz (160 samples) over calls of 2^22 samples: about
+    # 26k period spans per call, more than the span upload's one pass of
+    # 64 x 256 threads, from host inputs over both staging buffers
+    dm, fftpoint, count, calls, period, tb = 5.0, 4096, 2048, 2, 1e-5, 16
+    d = Dedisperser(BW, [dm], F0, fftpoint, count, series=False, precision=precision)
+    blk = d.block_samples
+    nd = int(d.Nd[0])
+    d.fold_init(period, BW, time_bin=tb, discard_Nd=nd)
+    o = O.Dedisp(BW, [dm], F0, fftpoint, count)
+    of = O.Fold(period, BW, blk, tb)
+    assert blk // of.period_samples > 64 * 256
+    of.discard_samples(nd)
+    x = u16(blk * calls, 7)
+    for c in range(calls):
+        part = x[c * blk:(c + 1) * blk]
+        d.filter_block(part)
+        of.fold_data(np.abs(o.filter(O.decode_uint16(part))[0]) ** 2)
+    ours = d.get_profiles()[0]
+    assert d.folded_periods() > 2 * 64 * 256
+    assert rel_rms(ours, of.fold_data_bins()) < (1e-5 if precision == "fp32" else 1e-4)
