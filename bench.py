@@ -975,7 +975,11 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
-def run_reference_gpu(args):
+def run_reference_gpu(args, sweep=False):
+    """The reference's own MSOSM_GPU_DM_concurrent on this GPU: the batched
+    workload (calls of 32 blocks), or with `sweep` the precision sweep's
+    64 MHz / FFT 8192 / DM 0-200 observation (calls of 8 blocks, the count
+    its ring allows at that depth)."""
     ws, rank, _ = dist_setup()
     if rank != 0:
         return
@@ -985,20 +989,27 @@ def run_reference_gpu(args):
         print(json.dumps({"impl": "reference-gpu", "unavailable": "oracle/_ref/ref_gpu_runner not built"}))
         return
     from msosm_gpu_b200 import simulate as S
+    if sweep:
+        bw, f0, fftpoint, dm_max, count, pul = (SWEEP["bw"], SWEEP["f0"], SWEEP["fftpoint"], SWEEP["dm_max"], 8,
+                                                SWEEP["pulsar"])
+    else:
+        bw, f0, fftpoint, dm_max, count, pul = BW, F0, FFTPOINT, DM_MAX, 32, PULSAR
     samples = 1 << args.log2_samples
-    # the reference leaves delays uninitialised at DM 0: trials (0, 100]
-    dms = ((np.arange(args.dms) + 1) * DM_MAX / args.dms).astype(np.float32)
-    x = make_signal(samples, on_gpu=False)
+    # the reference leaves delays uninitialised at DM 0: trials (0, dm_max]
+    dms = ((np.arange(args.dms) + 1) * dm_max / args.dms).astype(np.float32)
+    if sweep:
+        x = S.pulsar_baseband(samples, bw, f0, pul["dm"], pul["period"], pul["fwhm"], pul["snr"], seed=0)
+    else:
+        x = make_signal(samples, on_gpu=False)
     u = S.quantise_uint16(x, 1000.0)
-    count = 32
-    ncalls = samples // (count * FFTPOINT // 2)
+    ncalls = samples // (count * fftpoint // 2)
     with tempfile.TemporaryDirectory() as td:
         fin, fout = os.path.join(td, "in.u16"), os.path.join(td, "out.bin")
         u.tofile(fin)
         res = {}
         for with_out in (0, 1):
-            cmd = [O.REF_GPU_RUNNER, "time", str(FFTPOINT), str(count), str(ncalls), str(max(args.steps, 1)),
-                   str(with_out), str(BW), str(F0), fin, fout] + [repr(float(v)) for v in dms]
+            cmd = [O.REF_GPU_RUNNER, "time", str(fftpoint), str(count), str(ncalls), str(max(args.steps, 1)),
+                   str(with_out), str(bw), str(f0), fin, fout] + [repr(float(v)) for v in dms]
             r = subprocess.run(cmd, capture_output=True, text=True, timeout=1800)
             if r.returncode != 0:
                 print(json.dumps({"impl": "reference-gpu", "unavailable": f"runner exit {r.returncode}: "
@@ -1007,12 +1018,18 @@ def run_reference_gpu(args):
             ms = O.read_records(fout)["ms"]
             res[with_out] = float(np.median(ms))
     units = float(args.dms) * samples
-    print(json.dumps({"impl": "reference-gpu", "metric": METRIC, "unit": UNIT,
+    metric = ("DM-trial x Msamples/s (MS-OSM dedispersion, FFT %d, %d trials, 64 MHz precision-sweep "
+              "observation), 1 B200" % (fftpoint, args.dms)) if sweep else METRIC
+    print(json.dumps({"impl": "reference-gpu", "metric": metric, "unit": UNIT,
                       "value": units / (res[0] * 1e-3) / 1e6,
                       "value_with_series_d2h": units / (res[1] * 1e-3) / 1e6,
                       "ms_per_step": res[0], "ms_per_step_with_series_d2h": res[1], "steps": args.steps,
-                      "config": dict(workload_config(samples, args.dms, 1), dm_range_per_gpu=[float(dms[0]), DM_MAX],
-                                     count=count, input="uint16 offset binary (the reference API)"),
+                      "config": (dict(workload="precision-sweep observation: 64 MHz at 1400 MHz, 2^%d samples, "
+                                               "%d DM trials, FFT %d" % (args.log2_samples, args.dms, fftpoint),
+                                      samples_per_step=samples, dm_range=[float(dms[0]), dm_max], fftpoint=fftpoint,
+                                      count=count, input="uint16 offset binary (the reference API)") if sweep else
+                                 dict(workload_config(samples, args.dms, 1), dm_range_per_gpu=[float(dms[0]), DM_MAX],
+                                      count=count, input="uint16 offset binary (the reference API)")),
                       "method": "reference MSOSM_GPU_DM_concurrent (cuFFT + its kernels, sm_100a), "
                                 "std::chrono around filter_block_uint16 loop + synchronize, pinned host input "
                                 "(its own drivers' method); no folding (the reference has none for this class)"}),
@@ -1044,6 +1061,11 @@ def main():
     ap.add_argument("--obs", type=int, default=UNEVEN["n_obs"], help="uneven-batch: observations")
     ap.add_argument("--seeds", type=int, default=SWEEP["seeds"], help="precision-sweep: signal seeds")
     args = ap.parse_args()
+    if args.workload == "precision-sweep" and args.impl == "reference-gpu":
+        args.log2_samples = args.log2_samples or SWEEP["log2_samples"]
+        args.dms = args.dms or SWEEP["n_dm"]
+        run_reference_gpu(args, sweep=True)
+        return
     if args.workload != "batched":
         if args.impl != "ours":
             print(json.dumps({"impl": args.impl, "unavailable": f"the {args.workload} workload has no "
