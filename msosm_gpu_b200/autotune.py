@@ -15,6 +15,15 @@ Each candidate runs `calls` timed filter_block calls (after one warm-up) of
 about `sample` samples of device-resident noise, CUDA events on the handle's
 stream.  Results are cached per observation shape (and in a JSON file when
 ``cache_path`` is given).
+
+Every valid size gives the reference's MS-OSM result, but not the same one:
+the multi-segment approximation of the dispersion filter tightens as M grows.
+Measured against exact coherent dedispersion (classical overlap-save with the
+full-length filter) with the FP64 oracle, the coherence of the two outputs is
+rho ~ 1 - 0.24 sqrt(Nd) / M: 0.92 at the minimum FFT for 16 MHz at DM 100,
+0.875 for 64 MHz at DM 80, the loss halving with each doubling of M.  The
+fastest size is the least coherent, so ``min_coherence`` drops the sizes
+whose modelled coherence, for the trial of largest Nd, falls below it.
 """
 from __future__ import annotations
 
@@ -33,6 +42,16 @@ from .prepare import msosm_min_order as min_order_msosm, nd
 # on the 64 MHz / FFT 8192 precision sweep and the tensor-core parity tests)
 PROFILE_ERROR = {"fp32": 1e-6, "fp16": 3e-5, "bf16": 2e-3}
 TENSOR_SIZES = (4096, 8192)
+# 1 - rho = COHERENCE_SLOPE sqrt(Nd) / M, fitted to the FP64 oracle
+# (tests/test_msosm_coherence_cpu.py pins it within 25 %)
+COHERENCE_SLOPE = 0.24
+
+
+def coherence(bw: float, dm: float, f0: float, fftpoint: int) -> float:
+    """Modelled coherence of MS-OSM at this FFT size with exact coherent
+    dedispersion (0 .. 1)."""
+    M = int(fftpoint) // 2
+    return max(0.0, 1.0 - COHERENCE_SLOPE * math.sqrt(nd(bw, float(dm), f0)) / M)
 
 
 @dataclass
@@ -43,11 +62,20 @@ class Choice:
 
 
 def candidates(bw: float, dms: Sequence[float], f0: float, budget: float = 1e-3,
-               sizes: Sequence[int] = tuple(1 << k for k in range(11, 16))) -> List[Tuple[int, str]]:
-    """(fftpoint, precision) pairs worth timing for these trials."""
+               sizes: Sequence[int] = tuple(1 << k for k in range(11, 16)),
+               min_coherence: Optional[float] = None) -> List[Tuple[int, str]]:
+    """(fftpoint, precision) pairs worth timing for these trials; with
+    ``min_coherence`` only sizes whose modelled coherence (largest-Nd trial)
+    reaches it.  ValueError when no size does."""
     m_min = max(min_order_msosm(nd(bw, float(d), f0)) for d in dms)
     out = []
-    for n in sorted(set(max(int(s), 2 * m_min) for s in sizes)):
+    ns = sorted(set(max(int(s), 2 * m_min) for s in sizes))
+    if min_coherence is not None:
+        d_worst = max(float(d) for d in dms)
+        ns = [n for n in ns if coherence(bw, d_worst, f0, n) >= min_coherence]
+        if not ns:
+            raise ValueError(f"no FFT size of {list(sizes)} reaches coherence {min_coherence}")
+    for n in ns:
         out.append((n, "fp32"))
         if n in TENSOR_SIZES:
             for p in ("fp16", "bf16"):
@@ -56,10 +84,11 @@ def candidates(bw: float, dms: Sequence[float], f0: float, budget: float = 1e-3,
     return out
 
 
-def _key(bw, dms, f0, time_bin, budget, sizes) -> str:
+def _key(bw, dms, f0, time_bin, budget, sizes, min_coherence=None) -> str:
     d = np.asarray(dms, np.float64)
     return json.dumps([round(float(bw)), round(float(f0)), int(d.size), round(float(d.min()), 4),
-                       round(float(d.max()), 4), int(time_bin), budget, list(sizes)])
+                       round(float(d.max()), 4), int(time_bin), budget, list(sizes)]
+                      + ([] if min_coherence is None else [min_coherence]))
 
 
 class Autotuner:
@@ -97,12 +126,13 @@ class Autotuner:
             d.close()
 
     def tune(self, bw: float, dms: Sequence[float], f0: float, period: float = 0.0, time_bin: int = 1024,
-             budget: float = 1e-3, sizes: Sequence[int] = tuple(1 << k for k in range(11, 16))) -> Choice:
-        key = _key(bw, dms, f0, time_bin, budget, sizes)
+             budget: float = 1e-3, sizes: Sequence[int] = tuple(1 << k for k in range(11, 16)),
+             min_coherence: Optional[float] = None) -> Choice:
+        key = _key(bw, dms, f0, time_bin, budget, sizes, min_coherence)
         if key in self.cache:
             return Choice(**self.cache[key])
         best = None
-        for n, p in candidates(bw, dms, f0, budget, sizes):
+        for n, p in candidates(bw, dms, f0, budget, sizes, min_coherence):
             ms = self._time(bw, dms, f0, n, p, period, time_bin)
             self.log.append({"key": key, "fftpoint": n, "precision": p, "ms_per_msample": ms})
             if best is None or ms < best.ms_per_msample:

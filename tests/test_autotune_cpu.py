@@ -44,3 +44,17 @@ def test_uneven_observations():
         assert 16 <= o["trials"] <= 512 and 20 <= o["dm_max"] <= 300
         assert 0 < o["dm"] <= 0.9 * o["dm_max"] and 1e-3 <= o["period"] <= 1.0
     assert obs == bench.uneven_observations(64, 0)
+
+
+def test_coherence_floor_drops_the_coarsest_sizes():
+    from msosm_gpu_b200.autotune import candidates, coherence
+    bw, f0 = 16e6, 1242e6
+    dms = np.linspace(0.0, 100.0, 16)
+    all_sizes = sorted({n for n, _ in candidates(bw, dms, f0)})
+    assert all_sizes[0] == 2048
+    # FFT 2048 keeps ~0.92 of the exact filter's coherence at DM 100, 4096 ~0.96
+    assert 0.90 < coherence(bw, 100.0, f0, 2048) < 0.94 < coherence(bw, 100.0, f0, 4096) < 0.98
+    kept = sorted({n for n, _ in candidates(bw, dms, f0, min_coherence=0.95)})
+    assert kept == [n for n in all_sizes if n >= 4096]
+    with pytest.raises(ValueError):
+        candidates(bw, dms, f0, sizes=(2048,), min_coherence=0.95)
