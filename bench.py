@@ -702,7 +702,7 @@ def run_uneven_batch(args):
     import torch
     from msosm_gpu_b200 import Dedisperser
     from msosm_gpu_b200 import simulator as G
-    from msosm_gpu_b200.autotune import Autotuner, fixed_choice
+    from msosm_gpu_b200.autotune import Autotuner, coherence, fixed_choice
     from msosm_gpu_b200.prepare import nd
     cfg = UNEVEN
     obs = uneven_observations(args.obs, cfg["seed"])
@@ -714,7 +714,8 @@ def run_uneven_batch(args):
     for o in obs:
         dms = np.linspace(0.0, o["dm_max"], o["trials"]).astype(np.float32)
         t = time.time()
-        ch = tuner.tune(o["bw"], dms, o["f0"], period=o["period"], time_bin=cfg["nbins"])
+        ch = tuner.tune(o["bw"], dms, o["f0"], period=o["period"], time_bin=cfg["nbins"],
+                        min_coherence=args.min_coherence)
         tuning_s += time.time() - t
         tuned.append((ch.fftpoint, ch.precision))
         x = G.pulsar_baseband(o["n"], o["bw"], o["f0"], o["dm"], o["period"], o["duty"], o["snr"], seed=o["i"],
@@ -780,6 +781,8 @@ def run_uneven_batch(args):
                       "choices": {f"{n}/{p}": tuned.count((n, p)) for n, p in sorted(set(tuned))}},
             "fixed": fixed, "best_fixed": best, "tuned_vs_best_fixed": tuned_v / fixed[best]["value"],
             "tuning_s": tuning_s,
+            "min_coherence": args.min_coherence,
+            "tuned_coherence_min": min(coherence(o["bw"], o["dm_max"], o["f0"], n) for o, (n, _) in zip(obs, tuned)),
             "detected": {"rule": "best-S/N trial within max(1.5 trial steps, the DM error that smears one pulse "
                                  "width across the band) of the injected DM, over observations with >= 8 folded "
                                  "periods and an expected S/N >= 10",
@@ -1059,6 +1062,8 @@ def main():
     ap.add_argument("--eval", type=int, default=96, help="dm-proposal: held-out observations (half noise)")
     ap.add_argument("--snr-min", type=float, default=8.0, help="dm-proposal: sweep detection threshold")
     ap.add_argument("--obs", type=int, default=UNEVEN["n_obs"], help="uneven-batch: observations")
+    ap.add_argument("--min-coherence", type=float, default=None,
+                    help="uneven-batch: the autotuner's floor on MS-OSM coherence with exact dedispersion")
     ap.add_argument("--seeds", type=int, default=SWEEP["seeds"], help="precision-sweep: signal seeds")
     args = ap.parse_args()
     if args.workload == "precision-sweep" and args.impl == "reference-gpu":
