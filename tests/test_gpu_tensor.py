@@ -164,3 +164,49 @@ def test_fold_matches_oracle(precision, fft):
             f.fold_data(np.abs(ser[i, c * d.block_samples:(c + 1) * d.block_samples]) ** 2)
         e = rel_rms(prof[i], f.fold_data_bins())
         assert e < TOL[precision][1], (dms[i], e)
+
+
+@pytest.mark.parametrize("precision,fft,detect", [("fp16", 4096, "power"), ("fp16", 8192, "power"),
+                                                  ("fp16", 4096, "amplitude"), ("bf16", 8192, "power")])
+def test_series_and_fold_in_one_pass(precision, fft, detect):
+    # the kernel that writes the series and folds in the same pass: both
+    # outputs against the oracle, |y| as well as |y|^2 detection
+    dms, count, calls, period, tb = [0.0, 20.0, 73.2], 8 * 4096 // fft, 6, 0.0011, 256
+    d = Dedisperser(BW, dms, F0, fft, count, series=True, precision=precision)
+    nd = 4096
+    d.fold_init(period, BW, time_bin=tb, discard_Nd=nd, detect=detect)
+    o = O.Dedisp(BW, dms, F0, fft, count)
+    x = u16(d.block_samples * calls, 23)
+    ours, ser = [], []
+    for c in range(calls):
+        blk = x[c * d.block_samples:(c + 1) * d.block_samples]
+        d.filter_block(blk)
+        ours.append(d.get_output())
+        ser.append(o.filter(O.decode_uint16(blk)))
+    ours, ser = np.concatenate(ours, 1), np.concatenate(ser, 1)
+    prof = d.get_profiles()
+    assert d.folded_periods() > 0
+    for i in range(len(dms)):
+        assert rel_rms(ours[i], ser[i]) < TOL[precision][0], dms[i]
+        f = O.Fold(period, BW, d.block_samples, tb)
+        f.discard_samples(nd)
+        for c in range(calls):
+            y = ser[i, c * d.block_samples:(c + 1) * d.block_samples]
+            f.fold_data(np.abs(y) if detect == "amplitude" else np.abs(y) ** 2)
+        assert rel_rms(prof[i], f.fold_data_bins()) < TOL[precision][1], dms[i]
+
+
+def test_complex64_device_input_matches_uint16_host_input():
+    # the bench feeds complex64 already on the device; the same values as
+    # offset-binary host pairs give bit-identical series
+    import torch
+    dms, count, calls = [0.0, 30.0, 90.0], 4, 3
+    a = Dedisperser(BW, dms, F0, 4096, count, precision="fp16")
+    b = Dedisperser(BW, dms, F0, 4096, count, precision="fp16")
+    bs = a.block_samples
+    x = u16(bs * calls, 31)
+    xd = torch.from_numpy(O.decode_uint16(x).astype(np.complex64)).cuda()
+    for c in range(calls):
+        a.filter_block(x[c * bs:(c + 1) * bs])
+        b.filter_block(xd[c * bs:(c + 1) * bs])
+        assert np.array_equal(a.get_output(), b.get_output())
