@@ -45,8 +45,8 @@ def run_ref(args, inp):
         return O.read_records(fout)
 
 
-def ours(dms, fftpoint, count, x_u16, calls, osm=False):
-    d = Dedisperser(BW, dms, F0, fftpoint, count, osm=osm)
+def ours(dms, fftpoint, count, x_u16, calls, osm=False, precision="fp32"):
+    d = Dedisperser(BW, dms, F0, fftpoint, count, osm=osm, precision=precision)
     blk = d.block_samples
     out = []
     for c in range(calls):
@@ -71,6 +71,22 @@ def test_concurrent_matches_reference_gpu(fftpoint, count, dms):
     y, _ = ours(dms, fftpoint, count, x, calls)
     for i in range(len(dms)):
         assert rel_rms(y[i], ref[i]) < RTOL, (i, rel_rms(y[i], ref[i]))
+
+
+@pytest.mark.parametrize("fftpoint,count,dms", [(4096, 8, [0.5, 50.0, 73.2, 100.0]), (8192, 4, [150.0, 200.0])])
+def test_tensor_core_path_matches_reference_gpu(fftpoint, count, dms):
+    # the f16 tensor-core path against the reference's cuFFT path on the
+    # same input, within the tensor path's stated series error (1.5e-3)
+    calls = 6
+    M = fftpoint // 2
+    x = u16_noise(count * M * calls, 14)
+    r = run_ref(["concurrent", fftpoint, count, calls, BW, F0, "IN", "OUT"] + dms, x)
+    ref = r["out"].astype(np.float64).view(np.complex128).reshape(calls, len(dms), count * M)
+    ref = np.concatenate(list(ref), axis=1)
+    y, d = ours(dms, fftpoint, count, x, calls, precision="fp16")
+    assert d.fftpoint == fftpoint
+    for i in range(len(dms)):
+        assert rel_rms(y[i], ref[i]) < 1.5e-3, (dms[i], rel_rms(y[i], ref[i]))
 
 
 def test_single_dm_batch_matches_reference_gpu():
