@@ -86,7 +86,8 @@ MSOSM_API msosm_status msosm_prepare_segmentation(float bw, float dm, float f0, 
 
 /* Dedispersion filter H[2M] exactly as the reference designs it (chirp phase
  * in FP64 on the GPU, unnormalised M-point inverse DFT, zero pad, 2M-point
- * DFT; the extra factor M of the reference is kept).  Needs a GPU.
+ * DFT; the extra factor M of the reference is kept).  Needs a GPU.  dm < 0
+ * returns MSOSM_ERR_BAD_ARG, as msosm_dedisp_create does.
  * Replaces Prepare_MSOSM::generate_dedisp_params (msosm_prepare.cpp:37-84). */
 MSOSM_API msosm_status msosm_prepare_dedisp_params(float bw, float dm, float f0, unsigned long M,
                                          msosm_complex *H);
@@ -97,9 +98,11 @@ MSOSM_API msosm_status msosm_prepare_dedisp_params(float bw, float dm, float f0,
  * allocate while samples stream in, a host framework whose allocator owns the
  * device, code that redesigns one trial's filter in the middle of a pass
  * without the device-wide synchronisation cudaMalloc/cudaFree bring.
- * The caller passes H_device, a DEVICE buffer of 2M complex values; the
+ * The caller passes H_device, a DEVICE buffer of 2M complex values on the
+ * current device (memory of another device returns MSOSM_ERR_BAD_ARG); the
  * design runs asynchronously on `stream` (a cudaStream_t; NULL = the legacy
- * default stream) and writes H there, in the reference's scaling.
+ * default stream) and writes H there, in the reference's scaling.  Its
+ * arguments are checked as msosm_prepare_dedisp_params checks them.
  * M: a power of two, 32 <= M <= 8192 (FFT 64..16384 points); anything else
  * returns MSOSM_ERR_BAD_ARG.  Calls no cudaMalloc, cudaFree or allocating
  * library routine.  Scratch (twiddle tables, chirp parameters) lives in one

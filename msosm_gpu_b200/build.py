@@ -38,6 +38,15 @@ def headers():
                   + glob.glob(os.path.join(INCLUDE, "*.h")))
 
 
+OBJDIR = os.path.join(PKG, "_build")
+COMMON = ["-O3", "-std=c++17", *ARCH, "-lineinfo", "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
+          "-Xcompiler", "-fvisibility=hidden", "-I", INCLUDE, "-I", CSRC]
+
+
+def _obj(src: str) -> str:
+    return os.path.join(OBJDIR, os.path.basename(src) + ".o")
+
+
 def up_to_date() -> bool:
     if not os.path.exists(LIB):
         return False
@@ -46,21 +55,44 @@ def up_to_date() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False, ptxas_verbose: bool = False) -> str:
-    if not force and up_to_date():
+    """Compile each source to an object (in parallel; a source is recompiled
+    when it, any header or this script is newer than its object) and link
+    the shared library with the CUDA runtime linked in statically."""
+    if not force and not ptxas_verbose and up_to_date():
         return LIB
-    cmd = [nvcc(), "-O3", "-std=c++17", *ARCH, "-lineinfo", "-shared", "-cudart", "static",
-           "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off", "-Xcompiler", "-fvisibility=hidden",
-           "-I", INCLUDE, "-I", CSRC, "-o", LIB + ".tmp", *sources()]
-    if ptxas_verbose:
-        cmd[1:1] = ["-Xptxas", "-v"]
-    if verbose:
-        print(" ".join(cmd))
+    os.makedirs(OBJDIR, exist_ok=True)
+    newest_dep = max(os.path.getmtime(f) for f in headers() + [__file__])
+    flags = (["-Xptxas", "-v"] if ptxas_verbose else []) + COMMON
+
+    def stale(src: str) -> bool:
+        o = _obj(src)
+        return (force or ptxas_verbose or not os.path.exists(o)
+                or os.path.getmtime(o) < max(os.path.getmtime(src), newest_dep))
+
+    def compile_one(src: str):
+        cmd = [nvcc(), *flags, "-c", src, "-o", _obj(src) + ".tmp"]
+        if verbose:
+            print(" ".join(cmd))
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        if r.returncode == 0:
+            os.replace(_obj(src) + ".tmp", _obj(src))
+        return src, r
+
+    from concurrent.futures import ThreadPoolExecutor
+    todo = [s for s in sources() if stale(s)]
+    with ThreadPoolExecutor(max_workers=max(1, min(len(todo), os.cpu_count() or 4))) as ex:
+        results = list(ex.map(compile_one, todo))
+    failed = [(s, r) for s, r in results if r.returncode != 0]
+    for s, r in results:
+        if r.returncode != 0 or ptxas_verbose or verbose:
+            sys.stderr.write(r.stdout + r.stderr)
+    if failed:
+        raise RuntimeError("nvcc failed on " + ", ".join(os.path.basename(s) for s, _ in failed))
+    cmd = [nvcc(), *ARCH, "-shared", "-cudart", "static", "-o", LIB + ".tmp", *[_obj(s) for s in sources()]]
     r = subprocess.run(cmd, capture_output=True, text=True)
     if r.returncode != 0:
         sys.stderr.write(r.stdout + r.stderr)
-        raise RuntimeError("nvcc failed building libmsosm_b200.so")
-    if ptxas_verbose or verbose:
-        sys.stderr.write(r.stderr)
+        raise RuntimeError("nvcc failed linking libmsosm_b200.so")
     os.replace(LIB + ".tmp", LIB)
     return LIB
 

@@ -502,8 +502,8 @@ msosm_status msosm_prepare_segmentation(float bw, float dm, float f0, unsigned l
 
 msosm_status msosm_prepare_dedisp_params(float bw, float dm, float f0, unsigned long M, msosm_complex *H)
 {
-    if (!H || !(bw > 0) || !(f0 > 0))
-        return fail(MSOSM_ERR_BAD_ARG, "msosm_prepare_dedisp_params: bad arguments");
+    if (!H || !(bw > 0) || !(f0 > 0) || !(dm >= 0))
+        return fail(MSOSM_ERR_BAD_ARG, "msosm_prepare_dedisp_params: null output, or bw/f0 <= 0, or dm < 0");
     const int log2n = ilog2_exact(2 * M);
     if (log2n < 0)
         return fail(MSOSM_ERR_BAD_ARG, "M must be a power of two");

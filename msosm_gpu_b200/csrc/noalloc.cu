@@ -93,6 +93,11 @@ extern "C" MSOSM_API msosm_status msosm_prepare_dedisp_params_noalloc(float bw, 
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess)
         return fail(MSOSM_ERR_CUDA, "cudaGetDevice: %s", cudaGetErrorString(e));
+    // the design kernel runs on the current device and writes H there
+    if (at.type == cudaMemoryTypeDevice && at.device != dev)
+        return fail(MSOSM_ERR_BAD_ARG,
+                    "msosm_prepare_dedisp_params_noalloc: H is memory of device %d, the current device is %d",
+                    at.device, dev);
     if (dev < 0 || dev >= kMaxDevices)
         return fail(MSOSM_ERR_UNSUPPORTED, "device ordinal %d above %d", dev, kMaxDevices - 1);
     void *base = nullptr;

@@ -19,6 +19,17 @@ LIB_PATH = os.path.join(HERE, "_build", "liborc.so")
 REF_GOLDEN = os.path.join(HERE, "_ref", "ref_golden")
 REF_GPU_RUNNER = os.path.join(HERE, "_ref", "ref_gpu_runner")
 
+
+def reference_checkout() -> str | None:
+    """The msosm_gpu source tree the reference-side checkers are built from:
+    $MSOSM_REFERENCE, else a `reference` directory beside this repository;
+    None when neither holds the reference's sources."""
+    root = os.path.dirname(HERE)
+    for p in (os.environ.get("MSOSM_REFERENCE"), os.path.join(os.path.dirname(root), "reference")):
+        if p and os.path.isfile(os.path.join(p, "gpu", "gpu_kernel.cu")):
+            return p
+    return None
+
 _lib = None
 
 

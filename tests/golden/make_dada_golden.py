@@ -45,7 +45,10 @@ def file_bytes(case) -> bytes:
 
 
 def main() -> None:
-    subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "golden"], check=True)
+    ref = O.reference_checkout()
+    if not ref:
+        sys.exit("set MSOSM_REFERENCE to the msosm_gpu source tree")
+    subprocess.run(["make", "-C", os.path.join(ROOT, "oracle"), "golden", f"REF={ref}"], check=True)
     out = []
     with tempfile.TemporaryDirectory() as td:
         for i, c in enumerate(CASES):

@@ -59,8 +59,11 @@ def run(args):
 
 def main() -> None:
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=O.reference_checkout(),
+                    help="the msosm_gpu source tree (default: $MSOSM_REFERENCE, or `reference` beside the repo)")
     a = ap.parse_args()
+    if not a.ref:
+        ap.error("give --ref or set MSOSM_REFERENCE to the msosm_gpu source tree")
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "golden", f"REF={a.ref}"], check=True)
     meta = {"generator": "tests/golden/make_golden.py", "msosm": [], "osm": [], "fold": []}
     arrays = {}
