@@ -21,10 +21,12 @@ workload (`accuracy_vs_fp64`, in the CPU-baseline leg).
 `value`: device time (CUDA events) with the input resident in HBM.  `e2e`:
 the same metric through the C ABI with pinned HOST input, the host->device
 copy of every step and the device->host read of the folded profiles inside
-the timed region.  `--impl reference` times the oracle (the FP64 C
-restatement of the reference algorithm, OpenMP over trials) on the host
-cores on a bounded sample; `--impl reference-gpu` times the reference's own
-cuFFT classes built for sm_100a (oracle/_ref/ref_gpu_runner) when present.
+the timed region.  `--impl reference` times the reference's algorithm in
+FP32 on all host cores (oracle/cpu_fp32.py: pocketfft standing in for FFTW,
+threads over trials) on a bounded sample; `--impl reference-gpu` times the
+reference's own cuFFT classes built for sm_100a (oracle/_ref/ref_gpu_runner)
+when present, and the default arm carries that measurement as
+`reference_gpu` (run outside its timed region).
 
 `--workload precision-sweep` (not the bench line): a 64 MHz band centred at
 1400 MHz, 2^26 samples, 1024 trials over 0-200, FFT 8192, with an injected
@@ -176,36 +178,34 @@ class _NoClock:
 # ---------------------------------------------------------------------------
 
 def cpu_baseline(dms, x, budget_s=12.0):
+    """The reference's algorithm in FP32 on all host cores (oracle/cpu_fp32.py:
+    forward FFT, per-bin delayed filter product, inverse FFT, discard, |y|^2
+    and the Fold_GPU fold; pocketfft standing in for FFTW, threads over
+    trials), timed on a bounded sample of the workload."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    import oracle as O
+    import cpu_fp32 as C
     threads = os.cpu_count() or 1
-    O.lib().orc_set_threads(threads)
-    count = 8
-    d = O.Dedisp(BW, dms, F0, FFTPOINT, count, threads=threads)
-    blk = count * d.M
-    folds = [O.Fold(PULSAR["period"], BW, blk, NBINS) for _ in dms]
-    nd = int(max(d.Nd))
-    for f in folds:
-        f.discard_samples(nd)
+    count = 16
+    c = C.MsosmFP32(BW, dms, F0, FFTPOINT, count, period=PULSAR["period"], time_bin=NBINS, threads=threads)
+    blk = count * c.M
 
-    def one(c):
-        seg = x[(c * blk) % (x.size - blk):][:blk].astype(np.complex128)
-        y = d.filter(seg)
-        for i, f in enumerate(folds):
-            f.fold_data(np.abs(y[i]) ** 2)
+    def one(k):
+        c.filter(x[(k * blk) % (x.size - blk):][:blk])
 
     t = time.perf_counter()
     one(0)
     first = time.perf_counter() - t
-    calls = max(1, min(64, int(budget_s / max(first, 1e-3))))
+    calls = max(1, min(256, int(budget_s / max(first, 1e-3))))
     t = time.perf_counter()
-    for c in range(1, calls + 1):
-        one(c)
+    for k in range(1, calls + 1):
+        one(k)
     el = time.perf_counter() - t
+    c.close()
     v = len(dms) * calls * blk / el / 1e6
     return {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"{len(dms)} trials x {calls * blk} samples ({calls} calls of {blk}), FP64 oracle "
-                      f"(oracle/orc.c, radix-2 FFT, OpenMP over trials) incl. |y|^2 fold, {el:.1f} s"}
+            "sample": f"{len(dms)} trials x {calls * blk} samples ({calls} calls of {blk}): the reference's "
+                      f"MS-OSM in FP32 (oracle/cpu_fp32.py; {C.FFT_LIBRARY}), threads over trials, "
+                      f"incl. |y|^2 and the Fold_GPU fold, {el:.1f} s"}
 
 
 def accuracy_vs_fp64(dms, x, calls=48, count=8):
@@ -467,6 +467,14 @@ def run_ours(args):
     if rank == 0 and ws == 1 and not args.no_cpu:
         line["cpu_baseline"] = cpu_baseline(dms, x)
         line["accuracy_vs_fp64"] = accuracy_vs_fp64(dms, x)
+    if rank == 0 and ws == 1 and not args.no_reference_gpu:
+        # the reference's own cuFFT path on this GPU and this signal, after our
+        # timed regions (a separate process: its destructors reset the device)
+        rg = reference_gpu_measure(samples, args.dms, min(args.steps, 5), x=x, with_series=False)
+        if "value" in rg:
+            rg["our_e2e_over_this"] = e2e_v / rg["value"]
+            rg["our_value_over_this"] = value / rg["value"]
+        line["reference_gpu"] = rg
     de.close()
     if ws > 1:
         dist.barrier()
@@ -953,6 +961,205 @@ def run_dm_proposal(args):
 
 
 # ---------------------------------------------------------------------------
+# single DM: one trial through MS-OSM (FFT 4096) and OSM (FFT 2^18)
+# ---------------------------------------------------------------------------
+
+SINGLE = dict(bw=16e6, f0=1242e6, log2_samples=24, fftpoint=4096, osm_fftpoint=1 << 18, nbins=1024,
+              pulsar=dict(dm=50.0, period=5e-3, fwhm=0.02, snr=0.1), seed=0, call_log2=21, u16_scale=1000.0)
+
+
+def run_single_dm(args):
+    """One DM trial (16 MHz at 1250 MHz, 2^24 samples, pulsar P = 5 ms, 2 %
+    FWHM, peak SNR 0.1, DM 50, seed 0) through the MS-OSM path at FFT 4096
+    (FP32 and f16 tensor cores) and the OSM path at FFT 2^18, each folded
+    into 1024 bins; the same uint16 input through the reference's own
+    MSOSM_GPU_BATCH and OSM_GPU_BATCH (cuFFT, built for sm_100a) on the same
+    GPU, timed its own way; every series and profile against the FP64
+    oracle over the whole signal."""
+    import torch
+    from msosm_gpu_b200 import Dedisperser, simulate as S, simulator as G
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+
+    c = SINGLE
+    p = c["pulsar"]
+    bw, f0, nb = c["bw"], c["f0"], c["nbins"]
+    samples = 1 << (args.log2_samples or c["log2_samples"])
+    call = min(samples, 1 << c["call_log2"])
+    ncalls = samples // call
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    t = time.time()
+    x = G.pulsar_baseband(samples, bw, f0, p["dm"], p["period"], p["fwhm"], p["snr"], seed=c["seed"])
+    u = S.quantise_uint16(x, c["u16_scale"])
+    log(f"signal: {samples} samples in {time.time() - t:.1f} s, quantised to offset-binary uint16 "
+        f"({c['u16_scale']:.0f} counts per unit)")
+    ud = torch.from_numpy(u.view(np.int32).reshape(-1)).to(dev)
+    uh = torch.from_numpy(u.view(np.int32).reshape(-1)).pin_memory().numpy().view(np.uint16).reshape(-1, 2)
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(
+        os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    hbm = peaks.get("hbm_gbs")
+    uuid = None
+    try:
+        uuid = "GPU-" + str(torch.cuda.get_device_properties(dev).uuid)
+    except Exception:
+        pass
+    nd = O.nd(bw, p["dm"], f0)
+    paths = {"msosm_fp32": dict(fftpoint=c["fftpoint"], osm=False, precision="fp32"),
+             "msosm_fp16": dict(fftpoint=c["fftpoint"], osm=False, precision="fp16"),
+             "osm_fp32": dict(fftpoint=c["osm_fftpoint"], osm=True, precision="fp32")}
+
+    def handle(kw, count, series):
+        d = Dedisperser(bw, [p["dm"]], f0, kw["fftpoint"], count=count, osm=kw["osm"], series=series,
+                        precision=kw["precision"])
+        d.fold_init(p["period"], bw, time_bin=nb, discard_Nd=nd, detect="power")
+        return d
+
+    out = {}
+    series_of = {}
+    for name, kw in paths.items():
+        M = kw["fftpoint"] // 2
+        # device value: input resident, the whole signal in one call per step
+        # (series materialised and folded)
+        stream = torch.cuda.Stream(dev)
+        d = handle(kw, samples // M, True)
+        d.set_stream(stream)
+        for _ in range(args.warmup):
+            d.filter_block(ud)
+        torch.cuda.synchronize()
+        d.enable_timing(True)
+        with ClockSampler(uuid) as ck:
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(stream):
+                s.record(stream)
+                for _ in range(args.steps):
+                    d.filter_block(ud)
+                e.record(stream)
+            torch.cuda.synchronize()
+        ms = s.elapsed_time(e) / args.steps
+        tm = d.timing()
+        d.close()
+        k = max(tm["calls"], 1)
+        st = {"forward": tm["forward_ms"] / k, "dedisp": tm["dedisp_ms"] / k, "fold": tm["fold_ms"] / k}
+        # algorithmic bytes: uint16 input read once, complex64 series written once
+        algo = 12.0 * samples
+        kern_ms = st["forward"] + st["dedisp"]
+        # e2e through the C ABI from pinned host memory, calls of 2^21 samples:
+        # (a) fold only, the profile read back; (b) as the reference's drivers,
+        # every call's series copied back to pinned host memory
+        de = handle(kw, call // M, False)
+        ds = handle(kw, call // M, True)
+        ser = np.empty(call + 1, np.complex64)
+        ser = torch.from_numpy(ser.view(np.float32)).pin_memory().numpy().view(np.complex64)
+        keep = []
+
+        def e2e_fold():
+            for i in range(ncalls):
+                de.filter_block(uh[i * call:(i + 1) * call])
+            return de.get_profiles()
+
+        def e2e_series(collect=False):
+            for i in range(ncalls):
+                ds.filter_block(uh[i * call:(i + 1) * call])
+                ds.get_output(out=ser)
+                if collect:
+                    keep.append(ser[:-1].copy())
+            return ds.get_profiles()
+
+        e2e_series(collect=True)
+        series_of[name] = (np.concatenate(keep), ds.get_profiles()[0].copy())
+        res = {}
+        for key, fn in (("fold", e2e_fold), ("series", e2e_series)):
+            for _ in range(args.warmup):
+                fn()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(args.steps):
+                fn()
+            torch.cuda.synchronize()
+            res[key] = (time.perf_counter() - t0) / args.steps
+        de.close()
+        ds.close()
+        out[name] = {
+            "value": samples / (ms * 1e-3) / 1e6, "ms_per_step": ms, "unit": "Msamples/s (1 DM trial)",
+            "fftpoint": kw["fftpoint"], "precision": kw["precision"], "clocks": ck.summary(),
+            "stage_ms_per_step": st,
+            "roofline": {"bound": "hbm", "algorithmic_bytes_per_step": algo,
+                         "achieved": algo / (kern_ms * 1e-3) / 1e9, "peak": hbm, "unit": "GB/s",
+                         "frac": (algo / (kern_ms * 1e-3) / 1e9 / hbm) if hbm else None,
+                         "kernels": "forward + dedispersion kernels (uint16 input read, series written)"},
+            "e2e": {"value": samples / res["fold"] / 1e6, "unit": "Msamples/s (1 DM trial)",
+                    "ms_per_step": res["fold"] * 1e3, "h2d_bytes_per_step": int(u.nbytes),
+                    "d2h_bytes_per_step": nb * 4, "calls_per_step": ncalls},
+            "e2e_series": {"value": samples / res["series"] / 1e6, "unit": "Msamples/s (1 DM trial)",
+                           "ms_per_step": res["series"] * 1e3, "h2d_bytes_per_step": int(u.nbytes),
+                           "d2h_bytes_per_step": 8 * samples, "calls_per_step": ncalls}}
+        log(f"{name}: device {out[name]['value']:.0f} Msamples/s, e2e fold {out[name]['e2e']['value']:.0f}, "
+            f"e2e series {out[name]['e2e_series']['value']:.0f}")
+
+    # ---- errors against the FP64 oracle over the whole signal -------------
+    xin = O.decode_uint16(u)
+    for name, kw in paths.items():
+        M = kw["fftpoint"] // 2
+        o = O.Dedisp(bw, [p["dm"]], f0, kw["fftpoint"], call // M, osm=kw["osm"])
+        f = O.Fold(p["period"], bw, call, nb)
+        f.discard_samples(nd)
+        y, e2, r2 = [], 0.0, 0.0
+        ours, prof = series_of[name]
+        for i in range(ncalls):
+            yi = o.filter(xin[i * call:(i + 1) * call])[0]
+            f.fold_data(np.abs(yi) ** 2)
+            e2 += float(np.sum(np.abs(ours[i * call:(i + 1) * call] - yi) ** 2))
+            r2 += float(np.sum(np.abs(yi) ** 2))
+        pr = f.fold_data_bins()
+        out[name]["accuracy_vs_fp64"] = {
+            "series_rel_rms": math.sqrt(e2 / r2),
+            "profile_rel_rms": float(np.sqrt(np.sum((prof - pr) ** 2) / np.sum(pr ** 2))),
+            "sample": f"the whole signal ({samples} samples), FP64 oracle (oracle/orc.c)"}
+        snr_w = max(1, int(round(p["fwhm"] * nb)))
+        out[name]["profile_snr"] = profile_snr(prof, snr_w)
+
+    # ---- the reference's own single-DM classes on the same GPU and input ---
+    ref = {"unavailable": "oracle/_ref/ref_gpu_runner not built"}
+    if os.path.exists(O.REF_GPU_RUNNER):
+        ref = {}
+        with tempfile.TemporaryDirectory() as td:
+            fin, fout = os.path.join(td, "in.u16"), os.path.join(td, "out.bin")
+            u.tofile(fin)
+            for name, kind, fp in (("msosm_gpu_batch", "batch", c["fftpoint"]),
+                                   ("osm_gpu_batch", "osm", c["osm_fftpoint"])):
+                M = fp // 2
+                cmd = [O.REF_GPU_RUNNER, "time1", kind, str(fp), str(call // M), str(ncalls),
+                       str(max(args.steps, 1)), str(bw), repr(float(p["dm"])), str(f0), fin, fout, "1"]
+                r = subprocess.run(cmd, capture_output=True, text=True, timeout=1800)
+                if r.returncode != 0:
+                    ref[name] = {"unavailable": f"runner exit {r.returncode}: {r.stderr[-300:]}"}
+                    continue
+                rr = O.read_records(fout)
+                rms = float(np.median(rr["ms"]))
+                ys = rr["out"].astype(np.float64).view(np.complex128)
+                ref[name] = {"e2e": samples / (rms * 1e-3) / 1e6, "unit": "Msamples/s (1 DM trial)",
+                             "ms_per_step": rms, "count": call // M, "calls_per_step": ncalls,
+                             "method": "std::chrono around filter_block_uint16 + get_output(Complex*) per call "
+                                       "and a final synchronize, input and output cudaHostRegister'ed (the "
+                                       "reference's single-DM speed tests)"}
+                for ours_name in (("msosm_fp32", "msosm_fp16") if kind == "batch" else ("osm_fp32",)):
+                    a = series_of[ours_name][0].astype(np.complex128)
+                    ref[name]["series_rel_rms_vs_" + ours_name] = float(
+                        np.sqrt(np.sum(np.abs(a - ys) ** 2) / np.sum(np.abs(ys) ** 2)))
+    line = {"workload": "single-dm", "metric": "Msamples/s of one DM trial (MS-OSM FFT 4096, OSM FFT 2^18, "
+                                               "|y|^2 folded to 1024 bins), 1 B200",
+            "unit": "Msamples/s", "higher_is_better": True, "steps": args.steps, "warmup": args.warmup,
+            "data": "synthetic (seeded pulsar + AWGN from the device simulator, quantised to uint16)",
+            "config": {"workload": "single DM: 16 MHz @ 1250 MHz, 2^%d samples, pulsar P 5 ms, FWHM 2 %%, "
+                                   "peak SNR 0.1, DM 50, seed 0" % int(math.log2(samples)),
+                       "Nd": nd, "delaycount_fft4096": int(O.segmentation(bw, p["dm"], f0, c["fftpoint"] // 2)[0]),
+                       "call_samples": call, "fold_bins": nb, "input": "uint16 offset binary"},
+            "paths": out, "reference_gpu": ref}
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
 # reference arms
 # ---------------------------------------------------------------------------
 
@@ -972,71 +1179,79 @@ def run_reference(args):
     cb["value"] = v
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": None, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded pulsar + AWGN)",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded pulsar + AWGN)",
             "config": workload_config(samples, args.dms, ws), "cpu_baseline": cb,
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
-def run_reference_gpu(args, sweep=False):
-    """The reference's own MSOSM_GPU_DM_concurrent on this GPU: the batched
-    workload (calls of 32 blocks), or with `sweep` the precision sweep's
-    64 MHz / FFT 8192 / DM 0-200 observation (calls of 8 blocks, the count
-    its ring allows at that depth)."""
-    ws, rank, _ = dist_setup()
-    if rank != 0:
-        return
+def reference_gpu_measure(samples, n_dm, steps, sweep=False, x=None, with_series=True):
+    """The reference's own MSOSM_GPU_DM_concurrent (cuFFT + its kernels,
+    built for sm_100a into oracle/_ref/ref_gpu_runner) on this GPU, timed its
+    own way: the batched workload in calls of 32 blocks, or with `sweep` the
+    precision sweep's 64 MHz / FFT 8192 / DM 0-200 observation in calls of 8
+    blocks (the count its ring allows at that depth).  Trials (0, dm_max]:
+    the reference leaves its delays uninitialised at DM 0.  Returns a dict
+    (or one with "unavailable")."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle as O
     if not os.path.exists(O.REF_GPU_RUNNER):
-        print(json.dumps({"impl": "reference-gpu", "unavailable": "oracle/_ref/ref_gpu_runner not built"}))
-        return
+        return {"unavailable": "oracle/_ref/ref_gpu_runner not built"}
     from msosm_gpu_b200 import simulate as S
     if sweep:
         bw, f0, fftpoint, dm_max, count, pul = (SWEEP["bw"], SWEEP["f0"], SWEEP["fftpoint"], SWEEP["dm_max"], 8,
                                                 SWEEP["pulsar"])
     else:
         bw, f0, fftpoint, dm_max, count, pul = BW, F0, FFTPOINT, DM_MAX, 32, PULSAR
-    samples = 1 << args.log2_samples
-    # the reference leaves delays uninitialised at DM 0: trials (0, dm_max]
-    dms = ((np.arange(args.dms) + 1) * dm_max / args.dms).astype(np.float32)
-    if sweep:
-        x = S.pulsar_baseband(samples, bw, f0, pul["dm"], pul["period"], pul["fwhm"], pul["snr"], seed=0)
-    else:
-        x = make_signal(samples, on_gpu=False)
+    dms = ((np.arange(n_dm) + 1) * dm_max / n_dm).astype(np.float32)
+    if x is None:
+        if sweep:
+            x = S.pulsar_baseband(samples, bw, f0, pul["dm"], pul["period"], pul["fwhm"], pul["snr"], seed=0)
+        else:
+            x = make_signal(samples, on_gpu=False)
     u = S.quantise_uint16(x, 1000.0)
     ncalls = samples // (count * fftpoint // 2)
+    res = {}
     with tempfile.TemporaryDirectory() as td:
         fin, fout = os.path.join(td, "in.u16"), os.path.join(td, "out.bin")
         u.tofile(fin)
-        res = {}
-        for with_out in (0, 1):
-            cmd = [O.REF_GPU_RUNNER, "time", str(fftpoint), str(count), str(ncalls), str(max(args.steps, 1)),
+        del u
+        for with_out in ((0, 1) if with_series else (0,)):
+            cmd = [O.REF_GPU_RUNNER, "time", str(fftpoint), str(count), str(ncalls), str(max(steps, 1)),
                    str(with_out), str(bw), str(f0), fin, fout] + [repr(float(v)) for v in dms]
             r = subprocess.run(cmd, capture_output=True, text=True, timeout=1800)
             if r.returncode != 0:
-                print(json.dumps({"impl": "reference-gpu", "unavailable": f"runner exit {r.returncode}: "
-                                  f"{r.stderr[-300:]}"}))
-                return
-            ms = O.read_records(fout)["ms"]
-            res[with_out] = float(np.median(ms))
-    units = float(args.dms) * samples
+                return {"unavailable": f"runner exit {r.returncode}: {r.stderr[-300:]}"}
+            res[with_out] = float(np.median(O.read_records(fout)["ms"]))
+    units = float(n_dm) * samples
+    out = {"value": units / (res[0] * 1e-3) / 1e6, "unit": UNIT, "ms_per_step": res[0], "steps": steps,
+           "dm_range": [float(dms[0]), dm_max], "count": count, "fftpoint": fftpoint,
+           "input": "uint16 offset binary (the reference API), pinned host memory",
+           "method": "reference MSOSM_GPU_DM_concurrent (cuFFT + its kernels, sm_100a), std::chrono around "
+                     "the filter_block_uint16 loop + synchronize, pinned host input (its own drivers' "
+                     "method); host copies included; no folding (the reference has none for this class)"}
+    if 1 in res:
+        out["value_with_series_d2h"] = units / (res[1] * 1e-3) / 1e6
+        out["ms_per_step_with_series_d2h"] = res[1]
+    return out
+
+
+def run_reference_gpu(args, sweep=False):
+    """`--impl reference-gpu`: reference_gpu_measure as its own line."""
+    ws, rank, _ = dist_setup()
+    if rank != 0:
+        return
+    samples = 1 << args.log2_samples
+    m = reference_gpu_measure(samples, args.dms, args.steps, sweep=sweep)
+    if "unavailable" in m:
+        print(json.dumps({"impl": "reference-gpu", "unavailable": m["unavailable"]}))
+        return
     metric = ("DM-trial x Msamples/s (MS-OSM dedispersion, FFT %d, %d trials, 64 MHz precision-sweep "
-              "observation), 1 B200" % (fftpoint, args.dms)) if sweep else METRIC
-    print(json.dumps({"impl": "reference-gpu", "metric": metric, "unit": UNIT,
-                      "value": units / (res[0] * 1e-3) / 1e6,
-                      "value_with_series_d2h": units / (res[1] * 1e-3) / 1e6,
-                      "ms_per_step": res[0], "ms_per_step_with_series_d2h": res[1], "steps": args.steps,
-                      "config": (dict(workload="precision-sweep observation: 64 MHz at 1400 MHz, 2^%d samples, "
-                                               "%d DM trials, FFT %d" % (args.log2_samples, args.dms, fftpoint),
-                                      samples_per_step=samples, dm_range=[float(dms[0]), dm_max], fftpoint=fftpoint,
-                                      count=count, input="uint16 offset binary (the reference API)") if sweep else
-                                 dict(workload_config(samples, args.dms, 1), dm_range_per_gpu=[float(dms[0]), DM_MAX],
-                                      count=count, input="uint16 offset binary (the reference API)")),
-                      "method": "reference MSOSM_GPU_DM_concurrent (cuFFT + its kernels, sm_100a), "
-                                "std::chrono around filter_block_uint16 loop + synchronize, pinned host input "
-                                "(its own drivers' method); no folding (the reference has none for this class)"}),
-          flush=True)
+              "observation), 1 B200" % (SWEEP["fftpoint"], args.dms)) if sweep else METRIC
+    cfg = (dict(workload="precision-sweep observation: 64 MHz at 1400 MHz, 2^%d samples, %d DM trials, FFT %d"
+                         % (args.log2_samples, args.dms, SWEEP["fftpoint"]), samples_per_step=samples)
+           if sweep else dict(workload_config(samples, args.dms, 1)))
+    print(json.dumps(dict({"impl": "reference-gpu", "metric": metric, "config": cfg}, **m)), flush=True)
 
 
 def main():
@@ -1048,15 +1263,20 @@ def main():
     ap.add_argument("--log2-samples", type=int, default=None, help="default 26 for both workloads")
     ap.add_argument("--dms", type=int, default=None, help="default 256 (batched) or 1024 (precision-sweep)")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
+    ap.add_argument("--no-reference-gpu", action="store_true",
+                    help="skip the reference's cuFFT path in the default arm's line")
     ap.add_argument("--precision", default="fp16", choices=["fp32", "fp16", "bf16"],
                     help="inverse transforms on the CUDA cores (fp32) or the tensor cores (fp16, bf16)")
     ap.add_argument("--workload", default="batched",
-                    choices=["batched", "precision-sweep", "uneven-batch", "stream-to-file", "dm-proposal"],
+                    choices=["batched", "precision-sweep", "uneven-batch", "stream-to-file", "dm-proposal",
+                             "single-dm"],
                     help="batched: the 256-trial 16 MHz workload (the bench line); precision-sweep: the "
                          "64 MHz / FFT 8192 / 1024-trial sweep of the inverse-transform precisions; "
                          "uneven-batch: 64 independent observations, autotuned vs fixed configurations; "
                          "stream-to-file: host input in, every trial's uint16 series written to a file; "
-                         "dm-proposal: the learned coarse-DM proposal against the exhaustive fine sweep")
+                         "dm-proposal: the learned coarse-DM proposal against the exhaustive fine sweep; "
+                         "single-dm: one trial through MS-OSM (FFT 4096) and OSM (FFT 2^18) beside the "
+                         "reference's single-DM classes")
     ap.add_argument("--train", type=int, default=2048, help="dm-proposal: training samples")
     ap.add_argument("--epochs", type=int, default=40, help="dm-proposal: training epochs")
     ap.add_argument("--eval", type=int, default=96, help="dm-proposal: held-out observations (half noise)")
@@ -1077,7 +1297,8 @@ def main():
                               "reference arm"}))
             return
         {"precision-sweep": run_precision_sweep, "uneven-batch": run_uneven_batch,
-         "stream-to-file": run_stream_to_file, "dm-proposal": run_dm_proposal}[args.workload](args)
+         "stream-to-file": run_stream_to_file, "dm-proposal": run_dm_proposal,
+         "single-dm": run_single_dm}[args.workload](args)
         return
     args.log2_samples = args.log2_samples or LOG2_SAMPLES
     args.dms = args.dms or N_DM

@@ -1,0 +1,11 @@
+// fold_gpu.h -- include-name compatibility header for the reference's
+// folding/include/fold_gpu.h: the classes it declared, from the drop-in msosm_gpu_b200.hpp
+// (they run on libmsosm_b200.so), in the global namespace where the
+// reference's drivers look for them.
+#pragma once
+
+#include "globals.h"
+
+using msosm_b200::Fold_GPU;
+using msosm_b200::MSOSM_GPU_BATCH;
+using msosm_b200::OSM_GPU_BATCH;

@@ -1,0 +1,9 @@
+// osm_gpu_concurrent.h -- include-name compatibility header for the reference's
+// dedispersion/include/osm_gpu_concurrent.h: the classes it declared, from the drop-in msosm_gpu_b200.hpp
+// (they run on libmsosm_b200.so), in the global namespace where the
+// reference's drivers look for them.
+#pragma once
+
+#include "globals.h"
+
+using msosm_b200::OSM_GPU_DM_concurrent;

@@ -498,6 +498,18 @@ MSOSM_API msosm_status msosm_cnn_adam_step(msosm_cnn *n, float lr);
  * Diagnostics (no counterpart in the reference)
  * ====================================================================== */
 
+/* Limit of each wait of the tensor-core kernel (MSOSM_FLAG_TENSOR_*) on one
+ * of its GEMMs, in ns of the global timer; ns < 0 restores the default (1 s),
+ * 0 gives up at the first probe that finds a GEMM unfinished.  When a wait
+ * gives up, the kernel records a nonzero status, waits (1 s at most) for the
+ * GEMMs it still has in flight, frees its tensor memory and returns; the
+ * next synchronising call (get_output_*, get_profiles, synchronize) returns
+ * MSOSM_ERR_TIMEOUT and clears the status, and the handle carries on (the
+ * outputs of the calls since the previous check are invalid).  For tests of
+ * that path; returns MSOSM_ERR_STATE for a handle without the tensor-core
+ * kernel. */
+MSOSM_API msosm_status msosm_dedisp_set_tc_wait_limit(msosm_dedisp *d, long long ns);
+
 /* Runs one of the tensor-core GEMMs of MSOSM_FLAG_TENSOR_F16 on given data,
  * with the kernel's own shared-memory layouts, constant operand and
  * tensor-memory read-back: d = a * B_step, a a 128 x K matrix of f16 bit

@@ -16,18 +16,26 @@
 //  * reset_device() and the destructors release this object's resources
 //    only (the reference calls cudaDeviceReset, which ends every allocation
 //    of the process);
-//  * get_output() waits for the copy, so the wait_for_cpu / wait_for_threads
-//    handshake of the reference (a busy-wait on a plain bool,
-//    msosm_gpu_dm_concurrent.cpp:156-160) is kept as fields but never spins;
+//  * get_output() waits for the copy, so the wait_for_cpu flag of the
+//    reference (a busy-wait on a plain bool, msosm_gpu_dm_concurrent.cpp:
+//    156-160) is kept as a field but never spun on; get_output_thread keeps
+//    the hand-over to an output thread through wait_for_threads (atomic
+//    flags, a yielding wait bounded at 60 s);
+//  * copies of an object share its device handle (the reference's shallow
+//    copies share its device buffers);
 //  * trials with DM 0 get all block delays 0 (undefined in the reference).
 #pragma once
 
 #include <algorithm>
+#include <atomic>
+#include <chrono>
 #include <cstdio>
 #include <ctime>
 #include <cstdlib>
+#include <memory>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 #include "msosm_b200.h"
@@ -108,36 +116,19 @@ protected:
 
 namespace detail {
 
-// One msosm_dedisp handle plus the reference-shaped views of its state.
-class Handle {
-public:
-    Handle() = default;
-    Handle(const Handle &) = delete;
-    Handle &operator=(const Handle &) = delete;
-    ~Handle() { reset(); }
-    void create(const float *bw, const float *dm, const float *f0, int n, unsigned long fftpoint, int count,
-                unsigned long input_size, unsigned int flags)
-    {
-        reset();
-        check(msosm_dedisp_create(bw, dm, f0, n, fftpoint, count, input_size, flags, &h), "msosm_dedisp_create");
-        check(msosm_dedisp_get_info(h, &info), "msosm_dedisp_get_info");
-        n_ = n;
-        Nd.resize(n);
-        delaycount.resize(n);
-        check(msosm_dedisp_get_nd(h, Nd.data()), "msosm_dedisp_get_nd");
-        check(msosm_dedisp_get_delaycount(h, delaycount.data()), "msosm_dedisp_get_delaycount");
-        dp.assign((size_t)n * info.fftpoint, 0);
-        H.assign((size_t)n * info.fftpoint, Complex{0.f, 0.f});
-        for (int i = 0; i < n; ++i) {
-            check(msosm_dedisp_get_delay_points(h, i, dp.data() + (size_t)i * info.fftpoint), "delay_points");
-            check(msosm_dedisp_get_dedisp_params(h, i, H.data() + (size_t)i * info.fftpoint), "dedisp_params");
-        }
-    }
-    void reset()
+// One msosm_dedisp handle plus the reference-shaped views of its state,
+// shared by every copy of the object that holds it: the reference's classes
+// copy shallowly (their device buffers are shared by the copies, e.g. an
+// object passed by value to a thread, multiple_thread_osm.cpp:5-13), and so
+// do these.  The handle is destroyed with the last copy, or by reset().
+struct HandleState {
+    HandleState() = default;
+    HandleState(const HandleState &) = delete;
+    HandleState &operator=(const HandleState &) = delete;
+    ~HandleState()
     {
         if (h)
             msosm_dedisp_destroy(h);
-        h = nullptr;
     }
     size_t block() const { return (size_t)info.count * info.M; }
     Complex *device_output() const
@@ -156,6 +147,49 @@ public:
     std::vector<Complex> H;
 };
 
+class Handle {
+public:
+    void create(const float *bw, const float *dm, const float *f0, int n, unsigned long fftpoint, int count,
+                unsigned long input_size, unsigned int flags)
+    {
+        auto st = std::make_shared<HandleState>();
+        check(msosm_dedisp_create(bw, dm, f0, n, fftpoint, count, input_size, flags, &st->h),
+              "msosm_dedisp_create");
+        check(msosm_dedisp_get_info(st->h, &st->info), "msosm_dedisp_get_info");
+        st->n_ = n;
+        st->Nd.resize(n);
+        st->delaycount.resize(n);
+        check(msosm_dedisp_get_nd(st->h, st->Nd.data()), "msosm_dedisp_get_nd");
+        check(msosm_dedisp_get_delaycount(st->h, st->delaycount.data()), "msosm_dedisp_get_delaycount");
+        const unsigned long fp = st->info.fftpoint;
+        st->dp.assign((size_t)n * fp, 0);
+        st->H.assign((size_t)n * fp, Complex{0.f, 0.f});
+        for (int i = 0; i < n; ++i) {
+            check(msosm_dedisp_get_delay_points(st->h, i, st->dp.data() + (size_t)i * fp), "delay_points");
+            check(msosm_dedisp_get_dedisp_params(st->h, i, st->H.data() + (size_t)i * fp), "dedisp_params");
+        }
+        s_ = std::move(st);
+    }
+    // releases the device handle for every copy (the reference's reset_device
+    // resets the whole device)
+    void reset()
+    {
+        if (s_ && s_->h) {
+            msosm_dedisp_destroy(s_->h);
+            s_->h = nullptr;
+        }
+    }
+    HandleState *operator->() const
+    {
+        if (!s_)
+            check(MSOSM_ERR_STATE, "object used before initialize_uint16");
+        return s_.get();
+    }
+
+private:
+    std::shared_ptr<HandleState> s_;
+};
+
 }  // namespace detail
 
 // ---------------------------------------------------------------------------
@@ -169,29 +203,29 @@ public:
     void initialize_uint16(unsigned long fftpoint = 0, int count = 1)
     {
         h_.create(&bw_, &dm_, &f0_, 1, fftpoint, count, 0, extra_flags());
-        M = h_.info.M;
-        M_min = h_.info.M_min;
-        this->count = h_.info.count;
-        delaycount = h_.delaycount[0];
-        delay_points = h_.dp.data();
-        dedisp_params = h_.H.data();
-        output_buffer_d = h_.device_output();
+        M = h_->info.M;
+        M_min = h_->info.M_min;
+        this->count = h_->info.count;
+        delaycount = h_->delaycount[0];
+        delay_points = h_->dp.data();
+        dedisp_params = h_->H.data();
+        output_buffer_d = h_->device_output();
     }
     void filter_block_uint16(uint16_pair *input)
     {
-        check(msosm_dedisp_filter_block_uint16(h_.h, input), "filter_block_uint16");
+        check(msosm_dedisp_filter_block_uint16(h_->h, input), "filter_block_uint16");
     }
     void get_output(Complex *output)
     {
         // the handle's buffer ends with one extra element; copy count*M
-        out_.resize(h_.block() + 1);
-        check(msosm_dedisp_get_output_c64(h_.h, out_.data()), "get_output");
+        out_.resize(h_->block() + 1);
+        check(msosm_dedisp_get_output_c64(h_->h, out_.data()), "get_output");
         std::copy(out_.begin(), out_.end() - 1, output);
     }
 
     int count = 0;
     Complex *output_buffer_d = nullptr;
-    msosm_dedisp *handle() const { return h_.h; }
+    msosm_dedisp *handle() const { return h_->h; }
 
 protected:
     detail::Handle h_;
@@ -206,12 +240,12 @@ public:
     {
         (void)streaming;
         h_.create(&bw_, &dm_, &f0_, 1, fftpoint, count, 0, MSOSM_FLAG_OSM);
-        M = h_.info.M;
-        M_min = h_.info.M_min;
-        this->count = h_.info.count;
-        dedisp_params = h_.H.data();
-        output_buffer_d = h_.device_output();
-        total_memory = h_.info.device_bytes;
+        M = h_->info.M;
+        M_min = h_->info.M_min;
+        this->count = h_->info.count;
+        dedisp_params = h_->H.data();
+        output_buffer_d = h_->device_output();
+        total_memory = h_->info.device_bytes;
     }
     unsigned long total_memory = 0;
 };
@@ -222,61 +256,149 @@ public:
 
 class MSOSM_GPU_DM_concurrent {
 public:
+    // Prepare_MSOSM_DM_concurrent's constructor (msosm_prepare_dm_concurrent.cpp:3-29):
+    // the smear Nd of every trial; M, M_min, delaycount, dedisp_params and
+    // delay_points are allocated here and filled by the methods below or by
+    // initialize_uint16
     MSOSM_GPU_DM_concurrent(float *bw, float *dm, float *f0, int numDMs)
-        : numDMs(numDMs), bw_(bw, bw + numDMs), dm_(dm, dm + numDMs), f0_(f0, f0 + numDMs)
+        : numDMs(numDMs), bw_(bw, bw + numDMs), dm_(dm, dm + numDMs), f0_(f0, f0 + numDMs), nd_(numDMs, 0),
+          m_(numDMs, 0), m_min_(numDMs, 0), dc_(numDMs, 0), dp_ptr_(numDMs, nullptr), h_ptr_(numDMs, nullptr),
+          dp_own_(numDMs), h_own_(numDMs)
     {
+        for (int i = 0; i < numDMs; ++i)
+            check(msosm_prepare_nd(bw[i], dm[i], f0[i], &nd_[i]), "msosm_prepare_nd");
+        bind();
     }
+    MSOSM_GPU_DM_concurrent(const MSOSM_GPU_DM_concurrent &) = delete;
+    MSOSM_GPU_DM_concurrent &operator=(const MSOSM_GPU_DM_concurrent &) = delete;
     virtual ~MSOSM_GPU_DM_concurrent() = default;
     void get_device_info() { std::printf("CUDA devices: %d\n", msosm_device_count()); }
+
+    // --- Prepare_MSOSM_DM_concurrent (dedispersion/include/prepare_concurrent.h:10-38)
+    // per-trial minimum orders; M_common = M_common_min = their largest
+    // (msosm_prepare_dm_concurrent.cpp:31-49)
+    void calculate_min_order()
+    {
+        M_common = 0;
+        for (int i = 0; i < numDMs; ++i) {
+            check(osm_ ? msosm_prepare_min_order_osm(nd_[i], &m_[i]) : msosm_prepare_min_order_msosm(nd_[i], &m_[i]),
+                  "calculate_min_order");
+            m_min_[i] = m_[i];
+            M_common = std::max(M_common, m_[i]);
+        }
+        M_common_min = M_common;
+    }
+    void override_order(unsigned long order) { M_common = order; }
+    // trial i's filter at the common order (msosm_prepare_dm_concurrent.cpp:56-103)
+    void generate_dedisp_params(int i)
+    {
+        h_own_[i].assign(2 * M_common, Complex{0.f, 0.f});
+        check(msosm_prepare_dedisp_params(bw_[i], dm_[i], f0_[i], M_common, h_own_[i].data()),
+              "generate_dedisp_params");
+        h_ptr_[i] = h_own_[i].data();
+    }
+    // trial i's block delays at the common order (msosm_prepare_dm_concurrent.cpp:105-168)
+    void segmentation(int i)
+    {
+        dp_own_[i].assign(2 * M_common, 0);
+        check(msosm_prepare_segmentation(bw_[i], dm_[i], f0_[i], M_common, &dc_[i], dp_own_[i].data()),
+              "segmentation");
+        dp_ptr_[i] = dp_own_[i].data();
+    }
+
+    // --- MSOSM_GPU_DM_concurrent (dedispersion/include/msosm_gpu_concurrent.h:15-64)
     void initialize_uint16(unsigned long fftpoint, int count = 1, unsigned long input_size = 0,
                            bool compute_only = false)
     {
         create(fftpoint, count, input_size, extra_flags());
         this->compute_only = compute_only;
     }
-    void initialize_threads_flag(int thread_num) { wait_for_threads.assign(thread_num, false); }
+    void initialize_threads_flag(int thread_num)
+    {
+        threads_flag_.reset(new std::atomic<bool>[thread_num > 0 ? thread_num : 1]());
+        wait_for_threads = threads_flag_.get();
+    }
     void filter_block_uint16(uint16_pair *input)
     {
-        check(msosm_dedisp_filter_block_uint16(h_.h, input), "filter_block_uint16");
+        check(msosm_dedisp_filter_block_uint16(h_->h, input), "filter_block_uint16");
     }
     // numDMs*count*M + 1 elements, [dm][count*M] then a trailing zero
-    void get_output(Complex *output) { check(msosm_dedisp_get_output_c64(h_.h, output), "get_output"); }
+    void get_output(Complex *output) { check(msosm_dedisp_get_output_c64(h_->h, output), "get_output"); }
     void get_output(uint16_pair *output)
     {
-        check(msosm_dedisp_get_output_uint16(h_.h, output), "get_output");
+        check(msosm_dedisp_get_output_uint16(h_->h, output), "get_output");
     }
+    // The reference's hand-over to an output thread
+    // (msosm_gpu_dm_concurrent.cpp:182-195): unless compute_only, wait until
+    // that thread has taken the previous batch (it clears
+    // wait_for_threads[thread_id]), mark the slot taken, copy.  The wait
+    // yields instead of spinning on a plain bool and gives up after 60 s.
     void get_output_thread(uint16_pair *output, int thread_id)
     {
-        (void)thread_id;
+        if (!compute_only && wait_for_threads) {
+            const auto t0 = std::chrono::steady_clock::now();
+            while (wait_for_threads[thread_id].load(std::memory_order_acquire)) {
+                if (std::chrono::steady_clock::now() - t0 > std::chrono::seconds(60))
+                    check(MSOSM_ERR_TIMEOUT, "get_output_thread: the output thread did not take the last batch");
+                std::this_thread::yield();
+            }
+            wait_for_threads[thread_id].store(true, std::memory_order_release);
+        }
         get_output(output);
     }
-    void synchronize() { check(msosm_dedisp_synchronize(h_.h), "synchronize"); }
+    void synchronize() { check(msosm_dedisp_synchronize(h_->h), "synchronize"); }
     void reset_device() { h_.reset(); }
-    msosm_dedisp *handle() const { return h_.h; }
+    msosm_dedisp *handle() const { return h_->h; }
 
     int count = 0;
     bool wait_for_cpu = false;
-    std::vector<bool> wait_for_threads;
+    std::atomic<bool> *wait_for_threads = nullptr;  // one flag per output thread
     unsigned long M_common = 0, M_common_min = 0;
-    std::vector<unsigned long> Nd;
-    std::vector<int> delaycount;
+    // per trial (arrays of numDMs), as Prepare_MSOSM_DM_concurrent holds them
+    unsigned long *M = nullptr, *M_min = nullptr;
+    int *delaycount = nullptr;
+    Complex **dedisp_params = nullptr;  // [numDMs] -> 2*M_common filter values
+    int **delay_points = nullptr;       // [numDMs] -> 2*M_common block delays
+    unsigned long *Nd = nullptr;
     int numDMs;
-    // per-trial views (Prepare_MSOSM_DM_concurrent::delay_points / dedisp_params)
-    int *delay_points_of(int i) { return h_.dp.data() + (size_t)i * h_.info.fftpoint; }
-    Complex *dedisp_params_of(int i) { return h_.H.data() + (size_t)i * h_.info.fftpoint; }
+    // the same per-trial views by index
+    int *delay_points_of(int i) { return delay_points[i]; }
+    Complex *dedisp_params_of(int i) { return dedisp_params[i]; }
 
 protected:
     void create(unsigned long fftpoint, int count, unsigned long input_size, unsigned int flags)
     {
         h_.create(bw_.data(), dm_.data(), f0_.data(), numDMs, fftpoint, count, input_size, flags);
-        this->count = h_.info.count;
-        M_common = h_.info.M;
-        M_common_min = h_.info.M_min;
-        Nd = h_.Nd;
-        delaycount = h_.delaycount;
+        calculate_min_order();
+        this->count = h_->info.count;
+        M_common = h_->info.M;
+        M_common_min = h_->info.M_min;
+        for (int i = 0; i < numDMs; ++i) {
+            nd_[i] = h_->Nd[i];
+            dc_[i] = h_->delaycount[i];
+            dp_ptr_[i] = h_->dp.data() + (size_t)i * h_->info.fftpoint;
+            h_ptr_[i] = h_->H.data() + (size_t)i * h_->info.fftpoint;
+        }
+    }
+    void bind()
+    {
+        Nd = nd_.data();
+        M = m_.data();
+        M_min = m_min_.data();
+        delaycount = dc_.data();
+        delay_points = dp_ptr_.data();
+        dedisp_params = h_ptr_.data();
     }
     bool compute_only = false;
+    bool osm_ = false;  // Prepare_OSM_DM_concurrent's orders (osm_prepare_dm_concurrent.cpp)
     std::vector<float> bw_, dm_, f0_;
+    std::vector<unsigned long> nd_, m_, m_min_;
+    std::vector<int> dc_;
+    std::vector<int *> dp_ptr_;
+    std::vector<Complex *> h_ptr_;
+    std::vector<std::vector<int>> dp_own_;
+    std::vector<std::vector<Complex>> h_own_;
+    std::unique_ptr<std::atomic<bool>[]> threads_flag_;
     detail::Handle h_;
 };
 
@@ -286,6 +408,7 @@ public:
     using MSOSM_GPU_DM_concurrent::MSOSM_GPU_DM_concurrent;
     void initialize_uint16(unsigned long fftpoint = 0, int count = 1, bool compute_only = false)
     {
+        osm_ = true;
         create(fftpoint, count, 0, MSOSM_FLAG_OSM);
         this->compute_only = compute_only;
     }
@@ -306,25 +429,25 @@ public:
     void initialize_uint16(unsigned long fftpoint, int count = 1)
     {
         h_.create(bw_.data(), dm_.data(), f0_.data(), numOutput, fftpoint, count, 0, extra_flags());
-        this->count = h_.info.count;
-        M_loop = h_.info.M;
-        M_loop_min = h_.info.M_min;
-        Nd = h_.Nd;
-        delaycount = h_.delaycount;
+        this->count = h_->info.count;
+        M_loop = h_->info.M;
+        M_loop_min = h_->info.M_min;
+        Nd = h_->Nd;
+        delaycount = h_->delaycount;
     }
     // every trial is dedispersed here; filter_block_uint16(out, i) then
     // copies trial i (the reference runs trial i's filter at that point)
     void input_process(uint16_pair *input)
     {
-        check(msosm_dedisp_filter_block_uint16(h_.h, input), "input_process");
-        all_.resize((size_t)numOutput * h_.block() + 1);
-        check(msosm_dedisp_get_output_c64(h_.h, all_.data()), "get_output");
+        check(msosm_dedisp_filter_block_uint16(h_->h, input), "input_process");
+        all_.resize((size_t)numOutput * h_->block() + 1);
+        check(msosm_dedisp_get_output_c64(h_->h, all_.data()), "get_output");
     }
     void filter_block_uint16(Complex **output, int i)
     {
-        std::copy(all_.begin() + (size_t)i * h_.block(), all_.begin() + (size_t)(i + 1) * h_.block(), output[i]);
+        std::copy(all_.begin() + (size_t)i * h_->block(), all_.begin() + (size_t)(i + 1) * h_->block(), output[i]);
     }
-    void synchronize() { check(msosm_dedisp_synchronize(h_.h), "synchronize"); }
+    void synchronize() { check(msosm_dedisp_synchronize(h_->h), "synchronize"); }
 
     int count = 0;
     int numOutput;
@@ -350,25 +473,31 @@ public:
         create(fftpoint, count, 0, extra_flags());
         M_stream = M_common;
         M_stream_min = M_common_min;
+        flags_.reset(new bool[numStreams > 0 ? numStreams : 1]());
+        wait_for_cpu = flags_.get();
     }
     void get_output(Complex **output)
     {
         all_.resize((size_t)numStreams * block() + 1);
-        check(msosm_dedisp_get_output_c64(h_.h, all_.data()), "get_output");
+        check(msosm_dedisp_get_output_c64(h_->h, all_.data()), "get_output");
         for (int i = 0; i < numStreams; ++i)
             std::copy(all_.begin() + (size_t)i * block(), all_.begin() + (size_t)(i + 1) * block(), output[i]);
     }
     void get_output(uint16_pair **output)
     {
         u_.resize((size_t)numStreams * block() + 1);
-        check(msosm_dedisp_get_output_uint16(h_.h, u_.data()), "get_output");
+        check(msosm_dedisp_get_output_uint16(h_->h, u_.data()), "get_output");
         for (int i = 0; i < numStreams; ++i)
             std::copy(u_.begin() + (size_t)i * block(), u_.begin() + (size_t)(i + 1) * block(), output[i]);
     }
     int numStreams;
     unsigned long M_stream = 0, M_stream_min = 0;
+    // one flag per stream, as the reference's (msosm_gpu_batch_stream.h:73);
+    // get_output waits for its copy, so nothing spins on them
+    bool *wait_for_cpu = nullptr;
 
 private:
+    std::unique_ptr<bool[]> flags_;
     size_t block() const { return (size_t)count * M_common; }
     std::vector<Complex> all_;
     std::vector<uint16_pair> u_;
@@ -397,32 +526,32 @@ public:
         output_buffer_d.resize(numStreams);
         for (int i = 0; i < numStreams; ++i) {
             h_[i].create(&bw_[i], &dm_[i], &f0_[i], 1, fftpoint[i], count, 0, 0);
-            M[i] = h_[i].info.M;
-            M_min[i] = h_[i].info.M_min;
-            fftpoint[i] = h_[i].info.fftpoint;
-            Nd[i] = h_[i].Nd[0];
-            delaycount[i] = h_[i].delaycount[0];
-            output_buffer_d[i] = h_[i].device_output();
+            M[i] = h_[i]->info.M;
+            M_min[i] = h_[i]->info.M_min;
+            fftpoint[i] = h_[i]->info.fftpoint;
+            Nd[i] = h_[i]->Nd[0];
+            delaycount[i] = h_[i]->delaycount[0];
+            output_buffer_d[i] = h_[i]->device_output();
         }
         this->count = count;
     }
     void filter_block_uint16(uint16_pair **input)
     {
         for (int i = 0; i < numStreams; ++i)
-            check(msosm_dedisp_filter_block_uint16(h_[i].h, input[i]), "filter_block_uint16");
+            check(msosm_dedisp_filter_block_uint16(h_[i]->h, input[i]), "filter_block_uint16");
     }
     void get_output(Complex **output)
     {
         for (int i = 0; i < numStreams; ++i) {
-            out_.resize(h_[i].block() + 1);
-            check(msosm_dedisp_get_output_c64(h_[i].h, out_.data()), "get_output");
+            out_.resize(h_[i]->block() + 1);
+            check(msosm_dedisp_get_output_c64(h_[i]->h, out_.data()), "get_output");
             std::copy(out_.begin(), out_.end() - 1, output[i]);
         }
     }
     void synchronize()
     {
         for (auto &h : h_)
-            check(msosm_dedisp_synchronize(h.h), "synchronize");
+            check(msosm_dedisp_synchronize(h->h), "synchronize");
     }
 
     int count = 0;
@@ -453,6 +582,12 @@ public:
         folded_data = folded_.data();
         intensity_.assign(size, 0.f);
         total_intensity = intensity_.data();
+        count_.assign(period_samples, 0ul);
+        tmp_.assign(period_samples, 0.f);
+        fold_count = count_.data();
+        tmp_fold = tmp_.data();
+        period_ = period;
+        fs_ = fs;
     }
     Fold_GPU(const Fold_GPU &) = delete;
     Fold_GPU &operator=(const Fold_GPU &) = delete;
@@ -460,8 +595,14 @@ public:
     {
         if (h_)
             msosm_fold_destroy(h_);
+        if (planner_)
+            msosm_fold_planner_destroy(planner_);
     }
-    void discard_samples(unsigned long Nd) { check(msosm_fold_discard_samples(h_, Nd), "discard_samples"); }
+    void discard_samples(unsigned long Nd)
+    {
+        check(msosm_fold_discard_samples(h_, Nd), "discard_samples");
+        discard_ = Nd;
+    }
     // MSOSM_GPU_BATCH / OSM_GPU_BATCH: ordered after their last filter call
     void calculate_intensity(MSOSM_GPU_BATCH *pol1, MSOSM_GPU_BATCH *pol2)
     {
@@ -477,7 +618,12 @@ public:
     }
     // the host total_intensity buffer, after the caller filled it
     void load_total_intensity() { check(msosm_fold_set_intensity(h_, total_intensity), "set_intensity"); }
-    void fold_data() { check(msosm_fold_data(h_), "fold_data"); }
+    void fold_data()
+    {
+        check(msosm_fold_data(h_), "fold_data");
+        if (track_raw_state)
+            track_chunk();
+    }
     void fold_data_bins() { check(msosm_fold_data_bins(h_, folded_data), "fold_data_bins"); }
     void write_to_file()
     {
@@ -493,12 +639,53 @@ public:
     unsigned long time_bin = 0;
     float *total_intensity = nullptr;
     unsigned long period_samples = 0;
+    // Fold_GPU's raw-resolution state (fold_gpu.h:27-28), period_samples
+    // each: fold_count[p] counts the nonzero intensities folded at phase p
+    // (over every completed period; the reference counts only periods that
+    // lie inside one chunk, fold_gpu.cpp:124-132), tmp_fold holds the
+    // intensities of the period in progress.  The device fold needs neither,
+    // so they are kept only with track_raw_state set before the first
+    // fold_data (each chunk's intensities are then read back to the host).
+    unsigned long *fold_count = nullptr;
+    float *tmp_fold = nullptr;
+    bool track_raw_state = false;
 
 private:
+    // the chunk's destinations from the same fold state machine the device
+    // fold follows (msosm_fold_planner_chunk), applied to its intensities
+    void track_chunk()
+    {
+        if (!planner_)
+            check(msosm_fold_planner_create(period_, fs_, discard_, &planner_), "fold planner");
+        dest_.resize(size_);
+        unsigned long long done = 0;
+        check(msosm_fold_planner_chunk(planner_, size_, dest_.data(), &done), "fold planner");
+        check(msosm_fold_get_intensity(h_, total_intensity), "fold_data");
+        if (tmp_nz_.size() != period_samples)
+            tmp_nz_.assign(period_samples, 0);
+        for (unsigned long i = 0; i < size_; ++i) {
+            if (dest_[i] < 0)
+                continue;
+            const unsigned long ph = (unsigned long)(dest_[i] & 0xFFFFFFFFll);
+            tmp_fold[ph] = total_intensity[i];
+            tmp_nz_[ph] = total_intensity[i] != 0.f;
+            if (ph + 1 == period_samples)  // the period is complete
+                for (unsigned long p = 0; p < period_samples; ++p)
+                    fold_count[p] += tmp_nz_[p];
+        }
+    }
+
     msosm_fold *h_ = nullptr;
+    msosm_fold_planner *planner_ = nullptr;
     unsigned long size_;
     std::string outfile_;
     std::vector<float> folded_, intensity_;
+    std::vector<unsigned long> count_;
+    std::vector<float> tmp_;
+    std::vector<unsigned char> tmp_nz_;
+    std::vector<int64_t> dest_;
+    float period_ = 0.f, fs_ = 0.f;
+    unsigned long discard_ = 0;
 };
 
 // ---------------------------------------------------------------------------

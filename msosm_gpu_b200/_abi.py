@@ -121,6 +121,7 @@ def _declare(L: ctypes.CDLL) -> None:
         "msosm_dedisp_get_delay_points": (i32, [vp, i32, vp]),
         "msosm_dedisp_get_dedisp_params": (i32, [vp, i32, vp]),
         "msosm_dedisp_set_stream": (i32, [vp, vp]),
+        "msosm_dedisp_set_tc_wait_limit": (i32, [vp, ctypes.c_longlong]),
         "msosm_dedisp_filter_block_uint16": (i32, [vp, vp]),
         "msosm_dedisp_filter_block_c64": (i32, [vp, vp]),
         "msosm_dedisp_get_output_c64": (i32, [vp, vp]),

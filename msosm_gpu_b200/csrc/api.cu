@@ -89,6 +89,10 @@ cudaError_t dalloc(T **p, size_t count, size_t &total)
     return cudaMalloc((void **)p, count * sizeof(T) + 16);
 }
 
+// The tensor-core kernel's limit on each wait for one of its GEMMs (which
+// take microseconds): 1 s of global timer.
+constexpr long long kTcWaitLimitDefaultNs = 1000000000ll;
+
 }  // namespace
 
 namespace msosm {
@@ -135,6 +139,7 @@ struct msosm_dedisp {
     // a timed-out wait in the kernel
     bool tc = false, tc_bf16 = false;
     int *status_d = nullptr;
+    long long tc_wait_limit_ns = kTcWaitLimitDefaultNs;  // each wait of the kernel on a GEMM
     float *row_max = nullptr;  // [S] largest |component| of each ring row
     float *h_max = nullptr;    // [D] largest |component| of each trial's H
     int *delay_max_d = nullptr; // [D] largest block delay of each trial
@@ -838,6 +843,16 @@ msosm_status msosm_dedisp_set_stream(msosm_dedisp *d, void *stream)
     return MSOSM_OK;
 }
 
+msosm_status msosm_dedisp_set_tc_wait_limit(msosm_dedisp *d, long long ns)
+{
+    if (check_handle(d))
+        return fail(MSOSM_ERR_BAD_ARG, "null handle");
+    if (!d->tc)
+        return fail(MSOSM_ERR_STATE, "handle does not run the tensor-core kernel");
+    d->tc_wait_limit_ns = ns < 0 ? kTcWaitLimitDefaultNs : ns;
+    return MSOSM_OK;
+}
+
 // fold bookkeeping shared by both layouts: plan this call's spans, upload
 // them, flush a pending period that completes now, clear the partial rows
 static msosm_status fold_prepare(msosm_dedisp *d, int sb, FoldArgs &fa)
@@ -966,15 +981,19 @@ static msosm_status filter_block_large(msosm_dedisp *d, const void *src, InputKi
 }
 
 // After the handle's stream has drained: a timed-out wait of the
-// tensor-core kernel (its results are then invalid).
+// tensor-core kernel (the results of the calls since the last check are then
+// invalid).  The status word is cleared once reported, so the handle goes
+// on with the next call.
 static msosm_status kernel_status(msosm_dedisp *d)
 {
     if (!d->status_d)
         return MSOSM_OK;
     int st = 0;
     CK(cudaMemcpy(&st, d->status_d, sizeof(int), cudaMemcpyDeviceToHost));
-    if (st != 0)
+    if (st != 0) {
+        CK(cudaMemset(d->status_d, 0, sizeof(int)));
         return fail(MSOSM_ERR_TIMEOUT, "tensor-core kernel: a wait on the tensor core timed out");
+    }
     return MSOSM_OK;
 }
 
@@ -1047,6 +1066,7 @@ static msosm_status filter_block(msosm_dedisp *d, const void *input, InputKind k
     da.series = d->series_buf;
     da.fold.nspans = -1;
     da.status = d->status_d;
+    da.wait_limit_ns = d->tc_wait_limit_ns;
     da.row_max = d->row_max;
     da.h_max = d->h_max;
     da.delay_max = d->delay_max_d;

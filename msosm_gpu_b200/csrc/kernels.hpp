@@ -74,6 +74,7 @@ struct DedispArgs {
     FoldArgs fold;            // fold.nspans < 0: no folding
     // tensor-core kernel only
     int *status;              // nonzero after a timed-out wait
+    long long wait_limit_ns;  // limit of each wait on a GEMM (0: give up at the first incomplete probe)
     const float *row_max;     // [S] largest |component| of each ring row
     const float *h_max;       // [D] largest |component| of each trial's H
     const int *delay_max;     // [D] largest block delay of each trial

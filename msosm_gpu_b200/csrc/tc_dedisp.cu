@@ -76,9 +76,37 @@ __device__ __forceinline__ unsigned long long global_ns()
     return t;
 }
 
+// Probe without suspending: has the phase of the given parity completed?
+__device__ __forceinline__ bool mbar_test_wait(uint32_t bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
 // Waits for the phase of the given parity to complete; false after limit_ns.
+// A limit below the suspend hint probes without suspending, and a limit of
+// 0 gives up at the first probe that finds the phase incomplete (a
+// diagnostic setting: the kernel then takes its timeout exit).
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, unsigned long long limit_ns)
 {
+    if (limit_ns < kSuspendHintNs) {
+        if (mbar_test_wait(bar, parity))
+            return true;
+        if (limit_ns == 0)
+            return false;
+        const unsigned long long t0 = global_ns();
+        while (!mbar_test_wait(bar, parity))
+            if (global_ns() - t0 > limit_ns)
+                return false;
+        return true;
+    }
     if (mbar_try_wait(bar, parity))
         return true;
     const unsigned long long t0 = global_ns();
@@ -287,11 +315,12 @@ __device__ __forceinline__ void issue_gemm2(uint32_t tmem, uint32_t s0, uint32_t
 // Thread 0 waits for a commit (bounded); every thread learns the outcome.
 // Returns false (uniformly) on a timeout; parity then still names the
 // phase waited for.
-__device__ __forceinline__ bool wait_gemm(int tid, uint32_t bar, uint32_t &parity)
+__device__ __forceinline__ bool wait_gemm(int tid, uint32_t bar, uint32_t &parity,
+                                          unsigned long long limit_ns = kWaitLimitNs)
 {
     bool ok = true;
     if (tid == 0)
-        ok = mbar_wait(bar, parity, kWaitLimitNs);
+        ok = mbar_wait(bar, parity, limit_ns);
     const bool failed = __syncthreads_or(!ok);
     if (!failed)
         parity ^= 1;
@@ -353,6 +382,7 @@ __global__ void __launch_bounds__(TcShape<LOG2N>::THREADS, TcShape<LOG2N>::CTAS_
     const float2 *__restrict__ ring2 = a.ring;
     const int items = a.D * a.R;
     const int npairs = (a.count + 1) >> 1;
+    const unsigned long long wlim = (unsigned long long)a.wait_limit_ns;
     const int smask = a.S - 1;
     uint32_t phA = 0, phB = 0;
     bool pendA = false, pendB = false;  // a commit not yet waited for
@@ -556,7 +586,7 @@ __global__ void __launch_bounds__(TcShape<LOG2N>::THREADS, TcShape<LOG2N>::CTAS_
                 issue_gemm1<E, LOG2N>(tmem, s0, s0 + S::SMEM_OP0, barA);
             }
             pendA = true;
-            failed = !wait_gemm(tid, barA, phA);
+            failed = !wait_gemm(tid, barA, phA, wlim);
             if (!failed) {
                 pendA = false;
                 twiddle(opb);
@@ -584,7 +614,7 @@ __global__ void __launch_bounds__(TcShape<LOG2N>::THREADS, TcShape<LOG2N>::CTAS_
                     }
                     pendA = true;
                 }
-                if (!wait_gemm(tid, barB, phB)) {
+                if (!wait_gemm(tid, barB, phB, wlim)) {
                     failed = true;
                     break;
                 }
@@ -606,7 +636,7 @@ __global__ void __launch_bounds__(TcShape<LOG2N>::THREADS, TcShape<LOG2N>::CTAS_
                     }
                 }
                 if (more) {
-                    if (!wait_gemm(tid, barA, phA)) {
+                    if (!wait_gemm(tid, barA, phA, wlim)) {
                         failed = true;
                         break;
                     }

@@ -139,6 +139,13 @@ class Dedisperser:
         check(lib().msosm_dedisp_set_stream(self._h, ctypes.c_void_p(ptr)))
         self._stream_ptr = ptr
 
+    def set_tc_wait_limit(self, ns: int) -> None:
+        """Limit of each wait of the tensor-core kernel on a GEMM, in ns
+        (negative: the default 1 s; 0: give up at the first unfinished
+        probe).  A wait that gives up makes the next synchronising call raise
+        a timeout; the handle then carries on.  For tests of that path."""
+        check(lib().msosm_dedisp_set_tc_wait_limit(self._h, int(ns)))
+
     def filter_block(self, x) -> None:
         """Dedisperse the next count*M samples (host array or CUDA tensor)."""
         ptr, kind, keep = _input_pointer(x, self.block_samples)

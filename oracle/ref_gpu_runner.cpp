@@ -68,7 +68,9 @@ int usage()
                  "ref_gpu_runner fold2 <fftpoint> <count> <ncalls> <bw> <dm> <f0> <period> <time_bin>"
                  " <a.u16> <b.u16> <out>\n"
                  "ref_gpu_runner time <fftpoint> <count> <ncalls> <repeat> <with_output 0|1> <bw> <f0>"
-                 " <in.u16> <out> <dm...>\n");
+                 " <in.u16> <out> <dm...>\n"
+                 "ref_gpu_runner time1 <batch|osm> <fftpoint> <count> <ncalls> <repeat> <bw> <dm> <f0> <in.u16>"
+                 " <out> <write_series 0|1>\n");
     return 2;
 }
 
@@ -245,6 +247,69 @@ int main(int argc, char **argv)
         rec_u64("count", (uint64_t)m->count);
         rec("ms", "f8", ms.data(), ms.size(), 8);
         std::fclose(g_out);
+        std::_Exit(0);
+    }
+    if (mode == "time1" && argc == 13) {
+        // one DM through the single-trial classes, timed the way the
+        // reference's single-DM speed tests time them
+        // (test_processing_speed_msosm.cpp:198-221): input and output
+        // registered with cudaHostRegister, std::chrono around the
+        // filter_block_uint16 + get_output loop and a final synchronize.
+        // MSOSM_GPU_BATCH / OSM_GPU_BATCH copy with plain cudaMemcpy
+        // (msosm_gpu_batch.cpp:75-99, osm_gpu_batch.cpp:94-128).  The series
+        // of the first timed run is written out for the parity check.
+        const std::string kind = argv[2];
+        unsigned long fftpoint = std::strtoul(argv[3], nullptr, 10);
+        int count = std::atoi(argv[4]), ncalls = std::atoi(argv[5]), repeat = std::atoi(argv[6]);
+        float bw = std::strtof(argv[7], nullptr), dm = std::strtof(argv[8], nullptr),
+              f0 = std::strtof(argv[9], nullptr);
+        if (!nd_ok(bw, dm, f0) || (kind != "batch" && kind != "osm"))
+            return 5;
+        MSOSM_GPU_BATCH *ms = nullptr;
+        OSM_GPU_BATCH *os = nullptr;
+        unsigned long M = 0;
+        if (kind == "batch") {
+            ms = new MSOSM_GPU_BATCH(bw, dm, f0);
+            ms->initialize_uint16(fftpoint, count);
+            M = ms->M;
+        } else {
+            os = new OSM_GPU_BATCH(bw, dm, f0);
+            os->initialize_uint16(fftpoint, count, false);
+            M = os->M;
+        }
+        const size_t blk = (size_t)count * M;
+        std::vector<uint16_pair> in;
+        if (!read_u16(argv[10], in, blk * ncalls))
+            return 4;
+        std::vector<Complex> out(blk * ncalls);
+        if (cudaHostRegister(in.data(), in.size() * sizeof(uint16_pair), cudaHostRegisterDefault) != cudaSuccess ||
+            cudaHostRegister(out.data(), out.size() * sizeof(Complex), cudaHostRegisterDefault) != cudaSuccess)
+            return 6;
+        std::vector<double> ms_v;
+        for (int r = 0; r < repeat + 1; r++) {  // first run is warm-up
+            auto t0 = std::chrono::high_resolution_clock::now();
+            for (int c = 0; c < ncalls; c++) {
+                if (ms) {
+                    ms->filter_block_uint16(in.data() + c * blk);
+                    ms->get_output(out.data() + c * blk);
+                } else {
+                    os->filter_block_uint16(in.data() + c * blk);
+                    os->get_output(out.data() + c * blk);
+                }
+            }
+            cudaDeviceSynchronize();
+            auto t1 = std::chrono::high_resolution_clock::now();
+            if (r > 0)
+                ms_v.push_back(std::chrono::duration<double, std::milli>(t1 - t0).count());
+        }
+        g_out = std::fopen(argv[11], "wb");
+        rec_u64("M", M);
+        rec_u64("count", (uint64_t)count);
+        rec("ms", "f8", ms_v.data(), ms_v.size(), 8);
+        if (std::atoi(argv[12]))
+            rec("out", "f4", out.data(), 2 * out.size(), 4);
+        std::fclose(g_out);
+        std::fflush(stdout);
         std::_Exit(0);
     }
     return usage();

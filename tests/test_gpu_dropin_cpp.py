@@ -78,3 +78,35 @@ def test_dropin_classes_match_python_binding():
     np.testing.assert_array_equal(np.concatenate(streams[1]), py([3.5])[0])
     for i in range(3):
         np.testing.assert_array_equal(np.concatenate(loop[i]), conc[i])
+
+
+@pytest.mark.gpu
+def test_fold_raw_state_and_per_trial_prepare_fields():
+    import oracle as O
+    src = os.path.join(ROOT, "tests", "cpp", "fold_state_demo.cpp")
+    with tempfile.TemporaryDirectory() as td:
+        exe = os.path.join(td, "fold_state")
+        subprocess.run(["g++", "-std=c++17", "-O2", "-Wall", "-I", os.path.join(ROOT, "include"), "-o", exe, src,
+                        "-L", LIBDIR, "-lmsosm_b200", f"-Wl,-rpath,{LIBDIR}"], check=True, capture_output=True)
+        r = subprocess.run([exe], capture_output=True, text=True, timeout=300)
+    assert r.returncode == 0, r.stderr
+    lines = {l.split()[0]: l.split()[1:] for l in r.stdout.splitlines()}
+    ps = int(lines["period_samples"][0])
+    assert ps == 100
+    # 640 samples: periods 0..5 complete, 40 samples of period 6 in progress
+    t = np.arange(640)
+    val = np.where(t % 7 == 0, 0.0, 1.0 + t)
+    want_count = [(val[:600].reshape(6, 100)[:, p] != 0).sum() for p in range(100)]
+    assert [int(v) for v in lines["fold_count"]] == want_count
+    assert [float(v) for v in lines["tmp_fold"]] == list(val[600:640])
+    mins = [O.msosm_min_order(O.nd(16e6, dm, 1242e6)) for dm in (10.0, 50.0, 73.2)]
+    assert [int(v) for v in lines["M_min"][:3]] == mins and int(lines["M_min"][4]) == max(mins)
+    prep, hand = lines["prepared"], lines["handle"]
+    for dm_i, dm in enumerate((10.0, 50.0, 73.2)):
+        dc, dp = O.segmentation(16e6, dm, 1242e6, 2048)
+        assert int(prep[1 + dm_i]) == dc and int(hand[1 + dm_i]) == dc
+    assert int(prep[5]) == O.segmentation(16e6, 73.2, 1242e6, 2048)[1][100] == int(hand[5])
+    H = O.dedisp_params(16e6, 73.2, 1242e6, 2048)
+    for v in (prep, hand):
+        assert abs(complex(float(v[7]), float(v[8])) - H[7]) < 2e-5 * np.abs(H).max()
+    assert [int(v) for v in hand[10:13]] == mins and int(hand[14]) == O.nd(16e6, 73.2, 1242e6)

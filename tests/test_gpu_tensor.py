@@ -210,3 +210,35 @@ def test_complex64_device_input_matches_uint16_host_input():
         a.filter_block(x[c * bs:(c + 1) * bs])
         b.filter_block(xd[c * bs:(c + 1) * bs])
         assert np.array_equal(a.get_output(), b.get_output())
+
+
+@pytest.mark.parametrize("fftpoint", [4096, 8192])
+def test_wait_timeout_reports_and_handle_recovers(fftpoint):
+    # a wait limit of 0 makes the kernel's first wait on a GEMM give up: it
+    # takes its timeout exit (status word, drain of its own GEMMs, tensor
+    # memory freed) without hanging, the next synchronising call reports
+    # MSOSM_ERR_TIMEOUT, and after the default limit is restored the handle
+    # dedisperses its later calls exactly as the oracle does
+    from msosm_gpu_b200 import _abi
+    dms, count, calls = [10.0, 60.0], 6, 5
+    d = Dedisperser(BW, dms, F0, fftpoint, count, precision="fp16")
+    o = O.Dedisp(BW, dms, F0, fftpoint, count)
+    xs = [O.decode_uint16(u16(d.block_samples, 40 + c)).astype(np.complex64) for c in range(calls)]
+    d.filter_block(xs[0])
+    o.filter(xs[0].astype(np.complex128))
+    d.get_output()
+    d.set_tc_wait_limit(0)
+    d.filter_block(xs[1])
+    o.filter(xs[1].astype(np.complex128))
+    with pytest.raises(_abi.MsosmError) as ei:
+        d.get_output()
+    assert ei.value.status == _abi.ERR_TIMEOUT
+    d.set_tc_wait_limit(-1)
+    for c in range(2, calls):
+        d.filter_block(xs[c])
+        ref = o.filter(xs[c].astype(np.complex128))
+        y = d.get_output()
+        for i in range(len(dms)):
+            assert rel_rms(y[i], ref[i]) < SERIES_TOL, (c, i)
+    with pytest.raises(_abi.MsosmError):
+        Dedisperser(BW, dms, F0, fftpoint, count).set_tc_wait_limit(0)

@@ -107,3 +107,25 @@ def test_osm_batch_matches_reference_gpu():
     ref = r["out"].astype(np.float64).view(np.complex128)
     y, _ = ours([dm], 0, count, x, calls, osm=True)
     assert rel_rms(y[0], ref) < RTOL
+
+
+@pytest.mark.parametrize("precision,tol", [("fp32", RTOL), ("fp16", 1.5e-3)])
+def test_bench_scale_256_trials_match_reference_gpu(precision, tol):
+    # the bench's trial grid (256 trials over DM 0-100; the reference cannot
+    # run DM 0, so (0, 100]) at FFT 4096 in calls of 32 blocks, as its
+    # batch-32 speed test runs them (test_processing_speed_msosm_batch32_dm0to100.cpp)
+    calls, count, fftpoint, n = 3, 32, 4096, 256
+    M = fftpoint // 2
+    dms = [float(v) for v in ((np.arange(n) + 1) * 100.0 / n).astype(np.float32)]
+    x = u16_noise(count * M * calls, 21)
+    r = run_ref(["concurrent", fftpoint, count, calls, BW, F0, "IN", "OUT"] + [repr(v) for v in dms], x)
+    ref = r["out"].view(np.complex64).reshape(calls, n, count * M)
+    d = Dedisperser(BW, dms, F0, fftpoint, count, precision=precision)
+    worst = 0.0
+    for c in range(calls):
+        d.filter_block(x[c * count * M:(c + 1) * count * M])
+        y = d.get_output()
+        for i in range(n):
+            worst = max(worst, rel_rms(y[i].astype(np.complex128), ref[c, i].astype(np.complex128)))
+    d.close()
+    assert worst < tol, worst
