@@ -204,6 +204,41 @@ MSOSM_API msosm_status msosm_dedisp_get_output_uint16(msosm_dedisp *d, msosm_uin
 /* Device pointer of the series of the last call ([dm][count*M], complex). */
 MSOSM_API msosm_status msosm_dedisp_output_device_ptr(msosm_dedisp *d, msosm_complex **ptr);
 
+/* ---- batches: many observations in one launch ---------------------------
+ * One filter call of each of n handles (observations of any length, band
+ * and trial grid) with one persistent dedispersion launch per group of
+ * handles that run the same tensor-core kernel variant (FFT size, operand
+ * type, series/fold): the group's work items (handle, trial, block range)
+ * are taken by the CTAs from a counter, largest first, so uneven
+ * observations share the GPU without a tail per observation.  Handles of
+ * other kernels (FP32, FFT sizes without a tensor-core transform, the
+ * four-step sizes) run their calls one after another in the same batch call.
+ * The reference has no counterpart (it dedisperses one observation per
+ * object); its one-launch pattern for many trials of one observation is
+ * MSOSM_GPU_DM_concurrent::filter_block_uint16
+ * (dedispersion/msosm_dm_concurrent/msosm_gpu_dm_concurrent.cpp:119-151).
+ * msosm_batch_create puts every handle on the batch's stream (until the
+ * batch is destroyed); a handle belongs to one batch at a time.  inputs[i]
+ * holds count*M samples of handle i (host or device pointers), all of one
+ * kind.  Results per handle: msosm_dedisp_get_output_* / get_profiles, as
+ * after msosm_dedisp_filter_block_*; a handle's results equal those of its
+ * own calls up to the order of the fold's partial sums (the batch may cut a
+ * trial into fewer block ranges). */
+typedef struct msosm_batch msosm_batch;
+#define MSOSM_INPUT_UINT16 0
+#define MSOSM_INPUT_C64 1
+MSOSM_API msosm_status msosm_batch_create(msosm_dedisp *const *handles, int n, msosm_batch **out);
+MSOSM_API msosm_status msosm_batch_destroy(msosm_batch *b);
+MSOSM_API msosm_status msosm_batch_filter(msosm_batch *b, const void *const *inputs, int input_kind);
+/* Run the batch and its handles on a CUDA stream (a cudaStream_t; NULL =
+ * the batch's own). */
+MSOSM_API msosm_status msosm_batch_set_stream(msosm_batch *b, void *stream);
+/* Waits for the batch's work; MSOSM_ERR_TIMEOUT as msosm_dedisp_synchronize. */
+MSOSM_API msosm_status msosm_batch_synchronize(msosm_batch *b);
+/* Kernel groups, launches per call (groups + handles run alone), work items
+ * per call over the groups; any pointer may be NULL. */
+MSOSM_API msosm_status msosm_batch_get_info(const msosm_batch *b, int *groups, int *launches_per_call, int *items);
+
 /* ---- fused detection + folding ------------------------------------------
  * Folding follows Fold_GPU (folding/fold_gpu.cpp:3-194): period_samples =
  * (unsigned long)(period*fs), one sample skipped whenever the float drift
@@ -219,6 +254,13 @@ MSOSM_API msosm_status msosm_dedisp_fold_init(msosm_dedisp *d, float period, flo
 MSOSM_API msosm_status msosm_dedisp_get_profiles(msosm_dedisp *d, float *out);
 /* Number of whole periods folded so far. */
 MSOSM_API msosm_status msosm_dedisp_folded_periods(const msosm_dedisp *d, unsigned long long *n);
+
+/* Start a new input stream on the same handle (same band, trials and FFT):
+ * the previous stream's history is forgotten, as if the handle had just been
+ * created, and folding is unconfigured (call msosm_dedisp_fold_init again,
+ * with a new period if wanted).  No counterpart in the reference, whose
+ * objects serve one stream.  Waits for the handle's work. */
+MSOSM_API msosm_status msosm_dedisp_reset(msosm_dedisp *d);
 
 /* Wait for all work of the handle (MSOSM_GPU_DM_concurrent::synchronize). */
 MSOSM_API msosm_status msosm_dedisp_synchronize(msosm_dedisp *d);

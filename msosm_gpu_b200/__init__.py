@@ -8,6 +8,7 @@ face of that ABI; it has no compute path of its own.
 from ._abi import MsosmError, lib  # noqa: F401
 from .fold import Fold_GPU  # noqa: F401
 from .dedisp import (  # noqa: F401
+    DedispBatch,
     Dedisperser,
     MSOSM_GPU_BATCH,
     MSOSM_GPU_DM_concurrent,
@@ -16,6 +17,7 @@ from .dedisp import (  # noqa: F401
 )
 
 __all__ = [
+    "DedispBatch",
     "Dedisperser",
     "MSOSM_GPU_BATCH",
     "MSOSM_GPU_DM_concurrent",

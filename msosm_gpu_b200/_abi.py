@@ -33,6 +33,8 @@ SIM_TAG_PULSAR = 0
 SIM_TAG_AWGN = 1
 DETECT_POWER = 0
 DETECT_AMPLITUDE = 1
+INPUT_UINT16 = 0
+INPUT_C64 = 1
 
 
 class MsosmError(RuntimeError):
@@ -122,6 +124,13 @@ def _declare(L: ctypes.CDLL) -> None:
         "msosm_dedisp_get_dedisp_params": (i32, [vp, i32, vp]),
         "msosm_dedisp_set_stream": (i32, [vp, vp]),
         "msosm_dedisp_set_tc_wait_limit": (i32, [vp, ctypes.c_longlong]),
+        "msosm_dedisp_reset": (i32, [vp]),
+        "msosm_batch_create": (i32, [vp, i32, pvp]),
+        "msosm_batch_destroy": (i32, [vp]),
+        "msosm_batch_filter": (i32, [vp, vp, i32]),
+        "msosm_batch_synchronize": (i32, [vp]),
+        "msosm_batch_set_stream": (i32, [vp, vp]),
+        "msosm_batch_get_info": (i32, [vp, pi, pi, pi]),
         "msosm_dedisp_filter_block_uint16": (i32, [vp, vp]),
         "msosm_dedisp_filter_block_c64": (i32, [vp, vp]),
         "msosm_dedisp_get_output_c64": (i32, [vp, vp]),

@@ -997,24 +997,18 @@ static msosm_status kernel_status(msosm_dedisp *d)
     return MSOSM_OK;
 }
 
-static msosm_status filter_block(msosm_dedisp *d, const void *input, InputKind kind)
+// The first part of a filter call: the input staged (host inputs through a
+// device buffer on the copy stream), the forward transform into the ring,
+// the fold's spans for this call; da receives the dedispersion kernel's
+// arguments.  For the four-step layout the whole call runs here (*done).
+static msosm_status call_begin(msosm_dedisp *d, const void *input, InputKind kind, msosm_dedisp::CallEvents *ev,
+                               unsigned long long launches0, DedispArgs &da, bool &done)
 {
-    if (check_handle(d) || !input)
-        return fail(MSOSM_ERR_BAD_ARG, "null handle or input");
+    done = false;
     const size_t elem = kind == kInputU16 ? 4 : 8;
     const size_t bytes = (size_t)d->count * d->M * elem;
     const int sb = (int)(d->calls & 1);
     const void *src = input;
-    msosm_dedisp::CallEvents *ev = nullptr;
-    if (d->timing) {
-        msosm_dedisp::CallEvents c{};
-        for (cudaEvent_t &e : c.e)
-            CK(cudaEventCreate(&e));
-        c.h2d = false;
-        d->timed.push_back(c);
-        ev = &d->timed.back();
-    }
-    const unsigned long long launches0 = d->launches;
     if (!is_device_ptr(input)) {
         // stage through a device buffer on the copy stream; the host buffer
         // may be reused as soon as this call returns
@@ -1031,8 +1025,10 @@ static msosm_status filter_block(msosm_dedisp *d, const void *input, InputKind k
         CK(cudaStreamWaitEvent(d->stream, d->ev_copied[sb], 0));
         src = d->staging[sb];
     }
-    if (d->large)
+    if (d->large) {
+        done = true;
         return filter_block_large(d, src, kind, ev, launches0);
+    }
     FwdArgs fa{};
     fa.input = src;
     fa.hist_in = d->hist + (size_t)(d->calls & 1) * d->M;
@@ -1052,7 +1048,7 @@ static msosm_status filter_block(msosm_dedisp *d, const void *input, InputKind k
     if (ev)
         CK(cudaEventRecord(ev->e[1], d->stream));
 
-    DedispArgs da{};
+    da = DedispArgs{};
     da.ring = d->ring;
     da.S = d->S;
     da.max_delay = d->max_delay;
@@ -1075,6 +1071,46 @@ static msosm_status filter_block(msosm_dedisp *d, const void *input, InputKind k
         if (st != MSOSM_OK)
             return st;
     }
+    return MSOSM_OK;
+}
+
+// The last part of a filter call, after the dedispersion kernel: the ordered
+// reduction of the R partial profile rows, the series' trailing element.
+static msosm_status call_end(msosm_dedisp *d, msosm_dedisp::CallEvents *ev, int R, unsigned long long launches0)
+{
+    if (d->fold) {
+        CK(launch_fold_reduce(d->part_main, d->part_pend, d->D, R, d->nbins, d->acc_main, d->acc_pend, d->stream));
+        d->launches += 1;
+    }
+    if (d->series)
+        CK(cudaMemsetAsync(d->series_buf + (size_t)d->D * d->count * d->M, 0, sizeof(float2), d->stream));
+    if (ev) {
+        CK(cudaEventRecord(ev->e[6], d->stream));
+        d->timed_launches += d->launches - launches0;
+    }
+    d->calls += 1;
+    return MSOSM_OK;
+}
+
+static msosm_status filter_block(msosm_dedisp *d, const void *input, InputKind kind)
+{
+    if (check_handle(d) || !input)
+        return fail(MSOSM_ERR_BAD_ARG, "null handle or input");
+    msosm_dedisp::CallEvents *ev = nullptr;
+    if (d->timing) {
+        msosm_dedisp::CallEvents c{};
+        for (cudaEvent_t &e : c.e)
+            CK(cudaEventCreate(&e));
+        c.h2d = false;
+        d->timed.push_back(c);
+        ev = &d->timed.back();
+    }
+    const unsigned long long launches0 = d->launches;
+    DedispArgs da;
+    bool done = false;
+    msosm_status st = call_begin(d, input, kind, ev, launches0, da, done);
+    if (st != MSOSM_OK || done)
+        return st;
     // the partial-row clears and the flush above belong to the fold time;
     // the dedispersion kernel is timed alone
     if (ev)
@@ -1086,18 +1122,266 @@ static msosm_status filter_block(msosm_dedisp *d, const void *input, InputKind k
     d->launches += 1;
     if (ev)
         CK(cudaEventRecord(ev->e[3], d->stream));
-    if (d->fold) {
-        CK(launch_fold_reduce(d->part_main, d->part_pend, d->D, d->R, d->nbins, d->acc_main, d->acc_pend,
-                              d->stream));
-        d->launches += 1;
+    return call_end(d, ev, d->R, launches0);
+}
+
+// ---------------------------------------------------------------------------
+// batches: one filter call of many handles, one launch per kernel group
+// ---------------------------------------------------------------------------
+
+struct msosm_batch {
+    struct Group {
+        std::vector<int> members;  // handle indices, largest work items first
+        std::vector<int> R;        // block ranges per trial of each member in this batch
+        int log2n = 0;
+        bool bf16 = false, series = false, fold = false;
+        size_t fold_smem = 0;
+        int grid = 1;
+        int items = 0;
+        DedispArgs *args_d = nullptr;   // [n]
+        int *prefix_d = nullptr;        // [n + 1]
+        int *counter_d = nullptr;
+        DedispArgs *args_h = nullptr;   // pinned, [2][n]
+        cudaEvent_t ev_args[2] = {nullptr, nullptr};
+    };
+    std::vector<msosm_dedisp *> h;
+    std::vector<Group> groups;
+    std::vector<int> alone;  // handles launched one by one
+    cudaStream_t stream = nullptr;      // the stream everything runs on
+    cudaStream_t own_stream = nullptr;  // the batch's own (the default)
+    unsigned long long calls = 0;
+};
+
+static void batch_release(msosm_batch *b)
+{
+    if (!b)
+        return;
+    if (b->stream)
+        cudaStreamSynchronize(b->stream);
+    for (auto &g : b->groups) {
+        cudaFree(g.args_d);
+        cudaFree(g.prefix_d);
+        cudaFree(g.counter_d);
+        if (g.args_h)
+            cudaFreeHost(g.args_h);
+        for (cudaEvent_t e : g.ev_args)
+            if (e)
+                cudaEventDestroy(e);
     }
-    if (d->series)
-        CK(cudaMemsetAsync(d->series_buf + (size_t)d->D * d->count * d->M, 0, sizeof(float2), d->stream));
-    if (ev) {
-        CK(cudaEventRecord(ev->e[6], d->stream));
-        d->timed_launches += d->launches - launches0;
+    // the handles go back to their own streams
+    for (msosm_dedisp *d : b->h)
+        if (d->stream == b->stream)
+            d->stream = d->own_stream;
+    if (b->own_stream)
+        cudaStreamDestroy(b->own_stream);
+    delete b;
+}
+
+msosm_status msosm_batch_create(msosm_dedisp *const *handles, int n, msosm_batch **out)
+{
+    if (!out || !handles || n < 1)
+        return fail(MSOSM_ERR_BAD_ARG, "msosm_batch_create: null argument or n < 1");
+    *out = nullptr;
+    for (int i = 0; i < n; ++i) {
+        if (check_handle(handles[i]))
+            return fail(MSOSM_ERR_BAD_ARG, "msosm_batch_create: handle %d is null", i);
+        for (int j = 0; j < i; ++j)
+            if (handles[j] == handles[i])
+                return fail(MSOSM_ERR_BAD_ARG, "msosm_batch_create: handle %d appears twice", i);
     }
-    d->calls += 1;
+    msosm_batch *b = new (std::nothrow) msosm_batch;
+    if (!b)
+        return fail(MSOSM_ERR_OOM, "host allocation");
+    b->h.assign(handles, handles + n);
+#define CKB(call)                                                                                        \
+    do {                                                                                                 \
+        cudaError_t e_ = (call);                                                                         \
+        if (e_ != cudaSuccess) {                                                                         \
+            msosm_status s_ = cuda_fail(e_, #call);                                                      \
+            batch_release(b);                                                                            \
+            return s_;                                                                                   \
+        }                                                                                                \
+    } while (0)
+    CKB(cudaStreamCreateWithFlags(&b->own_stream, cudaStreamNonBlocking));
+    b->stream = b->own_stream;
+    int dev = 0, sms = 1;
+    CKB(cudaGetDevice(&dev));
+    CKB(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    for (int i = 0; i < n; ++i) {
+        msosm_dedisp *d = b->h[i];
+        // every handle's earlier work is done before the batch's stream takes over
+        CKB(cudaStreamSynchronize(d->stream));
+        d->stream = b->stream;
+        if (!d->tc || d->large) {
+            b->alone.push_back(i);
+            continue;
+        }
+        int gi = -1;
+        for (size_t k = 0; k < b->groups.size(); ++k) {
+            const auto &g = b->groups[k];
+            if (g.log2n == d->log2n && g.bf16 == d->tc_bf16 && g.series == d->series && g.fold == d->fold)
+                gi = (int)k;
+        }
+        if (gi < 0) {
+            b->groups.emplace_back();
+            gi = (int)b->groups.size() - 1;
+            auto &g = b->groups.back();
+            g.log2n = d->log2n;
+            g.bf16 = d->tc_bf16;
+            g.series = d->series;
+            g.fold = d->fold;
+        }
+        b->groups[gi].members.push_back(i);
+    }
+    for (auto &g : b->groups) {
+        // work items of similar size over the whole group: about eight per
+        // resident CTA, each member's block-pair ranges sized to that, never
+        // more ranges than the member's own partial rows hold
+        long long units = 0;
+        for (int i : g.members) {
+            const msosm_dedisp *d = b->h[i];
+            units += (long long)d->D * ((d->count + 1) / 2);
+            if (g.fold)
+                g.fold_smem = std::max(g.fold_smem, fold_smem_bytes(d->nbins, d->win_cap, d->nbins <= smem_bins_limit(d),
+                                                                    tc_threads(d->log2n)));
+        }
+        int per_sm = tc_blocks_per_sm(g.log2n, g.bf16, g.series, g.fold, g.fold_smem);
+        if (per_sm < 1)
+            per_sm = 1;
+        const long long resident = (long long)per_sm * sms;
+        const double per_item = std::max(1.0, (double)units / (8.0 * (double)resident));
+        // largest items first: the counter hands them out in this order
+        std::vector<std::pair<double, int>> order;
+        for (int i : g.members) {
+            const msosm_dedisp *d = b->h[i];
+            const long long pairs = (d->count + 1) / 2;
+            long long R = (long long)std::llround((double)pairs / per_item);
+            R = std::max(1ll, std::min(R, (long long)d->R));
+            order.push_back({(double)pairs / (double)R, i});
+        }
+        std::stable_sort(order.begin(), order.end(), [](const auto &x, const auto &y) { return x.first > y.first; });
+        g.members.clear();
+        std::vector<int> prefix(1, 0);
+        for (const auto &o : order) {
+            const msosm_dedisp *d = b->h[o.second];
+            const long long pairs = (d->count + 1) / 2;
+            const int R = (int)std::max(1ll, std::min((long long)d->R, (long long)std::llround((double)pairs / o.first)));
+            g.members.push_back(o.second);
+            g.R.push_back(R);
+            prefix.push_back(prefix.back() + d->D * R);
+        }
+        g.items = prefix.back();
+        g.grid = (int)std::min<long long>(g.items, resident);
+        const size_t nm = g.members.size();
+        CKB(cudaMalloc((void **)&g.args_d, sizeof(DedispArgs) * nm));
+        CKB(cudaMalloc((void **)&g.prefix_d, sizeof(int) * (nm + 1)));
+        CKB(cudaMalloc((void **)&g.counter_d, sizeof(int)));
+        CKB(cudaMallocHost((void **)&g.args_h, sizeof(DedispArgs) * 2 * nm));
+        CKB(cudaMemcpy(g.prefix_d, prefix.data(), sizeof(int) * (nm + 1), cudaMemcpyHostToDevice));
+        for (cudaEvent_t &e : g.ev_args)
+            CKB(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+#undef CKB
+    *out = b;
+    return MSOSM_OK;
+}
+
+msosm_status msosm_batch_destroy(msosm_batch *b)
+{
+    batch_release(b);
+    return MSOSM_OK;
+}
+
+msosm_status msosm_batch_get_info(const msosm_batch *b, int *groups, int *launches_per_call, int *items)
+{
+    if (!b)
+        return fail(MSOSM_ERR_BAD_ARG, "null batch");
+    if (groups)
+        *groups = (int)b->groups.size();
+    if (launches_per_call)
+        *launches_per_call = (int)(b->groups.size() + b->alone.size());
+    if (items) {
+        int t = 0;
+        for (const auto &g : b->groups)
+            t += g.items;
+        *items = t;
+    }
+    return MSOSM_OK;
+}
+
+msosm_status msosm_batch_filter(msosm_batch *b, const void *const *inputs, int input_kind)
+{
+    if (!b || !inputs)
+        return fail(MSOSM_ERR_BAD_ARG, "null batch or inputs");
+    if (input_kind != MSOSM_INPUT_UINT16 && input_kind != MSOSM_INPUT_C64)
+        return fail(MSOSM_ERR_BAD_ARG, "input_kind must be MSOSM_INPUT_UINT16 or MSOSM_INPUT_C64");
+    const InputKind kind = input_kind == MSOSM_INPUT_UINT16 ? kInputU16 : kInputC64;
+    for (size_t i = 0; i < b->h.size(); ++i)
+        if (!inputs[i])
+            return fail(MSOSM_ERR_BAD_ARG, "input %zu is null", i);
+    // handles outside every group: their whole call, one after another
+    for (int i : b->alone) {
+        msosm_status st = filter_block(b->h[i], inputs[i], kind);
+        if (st != MSOSM_OK)
+            return st;
+    }
+    const int sb = (int)(b->calls & 1);
+    for (auto &g : b->groups) {
+        const size_t nm = g.members.size();
+        // the pinned argument staging of two calls ago has been copied
+        CK(cudaEventSynchronize(g.ev_args[sb]));
+        DedispArgs *ah = g.args_h + (size_t)sb * nm;
+        std::vector<unsigned long long> l0(nm);
+        for (size_t j = 0; j < nm; ++j) {
+            msosm_dedisp *d = b->h[g.members[j]];
+            l0[j] = d->launches;
+            bool done = false;
+            msosm_status st = call_begin(d, inputs[g.members[j]], kind, nullptr, l0[j], ah[j], done);
+            if (st != MSOSM_OK)
+                return st;
+            ah[j].R = g.R[j];
+        }
+        CK(cudaMemcpyAsync(g.args_d, ah, sizeof(DedispArgs) * nm, cudaMemcpyHostToDevice, b->stream));
+        CK(cudaEventRecord(g.ev_args[sb], b->stream));
+        CK(cudaMemsetAsync(g.counter_d, 0, sizeof(int), b->stream));
+        BatchArgs ba{};
+        ba.args = g.args_d;
+        ba.prefix = g.prefix_d;
+        ba.nobs = (int)nm;
+        ba.counter = g.counter_d;
+        CK(launch_tc_dedisp_batch(g.log2n, g.bf16, g.series, g.fold, ba, g.fold_smem, g.grid, b->stream));
+        for (size_t j = 0; j < nm; ++j) {
+            msosm_dedisp *d = b->h[g.members[j]];
+            msosm_status st = call_end(d, nullptr, g.R[j], l0[j]);
+            if (st != MSOSM_OK)
+                return st;
+        }
+    }
+    b->calls += 1;
+    return MSOSM_OK;
+}
+
+msosm_status msosm_batch_set_stream(msosm_batch *b, void *stream)
+{
+    if (!b)
+        return fail(MSOSM_ERR_BAD_ARG, "null batch");
+    CK(cudaStreamSynchronize(b->stream));
+    b->stream = stream ? (cudaStream_t)stream : b->own_stream;
+    for (msosm_dedisp *d : b->h)
+        d->stream = b->stream;
+    return MSOSM_OK;
+}
+
+msosm_status msosm_batch_synchronize(msosm_batch *b)
+{
+    if (!b)
+        return fail(MSOSM_ERR_BAD_ARG, "null batch");
+    CK(cudaStreamSynchronize(b->stream));
+    for (msosm_dedisp *d : b->h) {
+        msosm_status st = kernel_status(d);
+        if (st != MSOSM_OK)
+            return st;
+    }
     return MSOSM_OK;
 }
 
@@ -1220,6 +1504,55 @@ msosm_status msosm_dedisp_fold_init(msosm_dedisp *d, float period, float fs, uns
     CK(cudaMemsetAsync(d->acc_pend, 0, sizeof(double) * nacc, d->stream));
     CK(cudaStreamSynchronize(d->stream));
     d->fold = true;
+    return MSOSM_OK;
+}
+
+// Frees what fold_init allocated and forgets the fold configuration.
+static void fold_free(msosm_dedisp *d)
+{
+    void *bufs[] = {d->part_main, d->part_pend, d->acc_main, d->acc_pend, d->prof_out,
+                    d->span_a_d, d->span_b_d, d->span_p_d, d->span_dest_d, d->lI};
+    for (void *p : bufs)
+        if (p)
+            cudaFree(p);
+    if (d->span_host)
+        cudaFreeHost(d->span_host);
+    const size_t prow = (size_t)d->D * d->R * d->nbins, nacc = (size_t)d->D * d->nbins;
+    size_t freed = 2 * prow * sizeof(float) + 2 * nacc * sizeof(double) + nacc * sizeof(float) +
+                   (size_t)d->span_cap * (2 * sizeof(long long) + 2 * sizeof(int));
+    if (d->large)
+        freed += (size_t)d->D * d->count * d->M * sizeof(float);
+    d->device_bytes = d->device_bytes > freed ? d->device_bytes - freed : 0;
+    d->part_main = d->part_pend = d->prof_out = d->lI = nullptr;
+    d->acc_main = d->acc_pend = nullptr;
+    d->span_a_d = d->span_b_d = nullptr;
+    d->span_p_d = d->span_dest_d = nullptr;
+    d->span_host = nullptr;
+    delete d->planner;
+    d->planner = nullptr;
+    d->fold = false;
+}
+
+msosm_status msosm_dedisp_reset(msosm_dedisp *d)
+{
+    if (check_handle(d))
+        return fail(MSOSM_ERR_BAD_ARG, "null handle");
+    CK(cudaStreamSynchronize(d->stream));
+    CK(cudaStreamSynchronize(d->copy_stream));
+    // the kernels read no ring row of a block before the stream start, so a
+    // new stream needs only the zero history of its first window
+    CK(cudaMemset(d->hist, 0, sizeof(float2) * 2 * d->M));
+    d->calls = 0;
+    if (d->fold)
+        fold_free(d);
+    if (d->status_d)
+        CK(cudaMemset(d->status_d, 0, sizeof(int)));
+    if (!d->large) {
+        // the grid the handle had before fold_init
+        cudaError_t e = plan_grid(d);
+        if (e != cudaSuccess)
+            return cuda_fail(e, "plan_grid");
+    }
     return MSOSM_OK;
 }
 

@@ -80,6 +80,17 @@ struct DedispArgs {
     const int *delay_max;     // [D] largest block delay of each trial
 };
 
+// One launch over the work items of many handles (observations) that run the
+// same kernel variant: handle o's items are [prefix[o], prefix[o + 1]), each
+// with args[o]; a CTA takes the next item from *counter (zero before the
+// launch), so items of uneven size balance over the grid.
+struct BatchArgs {
+    const DedispArgs *args;  // [nobs], device memory
+    const int *prefix;       // [nobs + 1], device memory
+    int nobs;
+    int *counter;
+};
+
 struct DesignArgs {
     const ChirpParams *chirp;  // [D] device
     int D;
@@ -132,6 +143,10 @@ int tc_blocks_per_sm(int log2n, bool bf16, bool series, bool fold, size_t extra_
 // (else f16)
 cudaError_t launch_tc_dedisp(int log2n, bool bf16, bool series, bool fold, const DedispArgs &a, int grid,
                              cudaStream_t st);
+// the same over the items of several handles in one launch (a batch);
+// fold_smem: the largest fold shared-memory size over the handles
+cudaError_t launch_tc_dedisp_batch(int log2n, bool bf16, bool series, bool fold, const BatchArgs &b,
+                                   size_t fold_smem, int grid, cudaStream_t st);
 // rows of 2^log2n bins from natural into tensor-core order (out of place)
 cudaError_t launch_tc_permute_rows(const float2 *in, float2 *out, int rows, int log2n, cudaStream_t st);
 // one GEMM of the kernel on given data: a = 128 x K f16 bit patterns

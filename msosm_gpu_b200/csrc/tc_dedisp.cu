@@ -338,9 +338,9 @@ __device__ __forceinline__ void pow2_scale_to(float mx, float &s, float &inv)
     inv = __int_as_float((e - X + 1) << 23);
 }
 
-template <int LOG2N, class E, bool SERIES, bool FOLD>
+template <int LOG2N, class E, bool SERIES, bool FOLD, bool MULTI>
 __global__ void __launch_bounds__(TcShape<LOG2N>::THREADS, TcShape<LOG2N>::CTAS_PER_SM)
-    tc_dedisp_kernel(DedispArgs a)
+    tc_dedisp_kernel(DedispArgs a0, BatchArgs bt)
 {
     using S = TcShape<LOG2N>;
     constexpr int N = S::N, M = S::M, N2 = S::N2, W = S::WARPS, T = S::THREADS;
@@ -349,8 +349,8 @@ __global__ void __launch_bounds__(TcShape<LOG2N>::THREADS, TcShape<LOG2N>::CTAS_
     const uint32_t s0 = smem_addr(sm);
     const uint32_t barA = s0 + S::SMEM_CTL, barB = s0 + S::SMEM_CTL + 8;
     FoldSmem fw;
-    if constexpr (FOLD)
-        fold_smem_layout(fw, sm + S::SMEM_FOLD, a.fold);
+    if constexpr (FOLD && !MULTI)
+        fold_smem_layout(fw, sm + S::SMEM_FOLD, a0.fold);
     fill_constants<E, LOG2N>(sm, tid);
     const uint32_t tmem = tc_setup<LOG2N>(sm, s0, tid, warp);
     // epilogue view: warp w reads TMEM lanes 32 (w % 4) .. + 31 (its GEMM
@@ -378,16 +378,28 @@ __global__ void __launch_bounds__(TcShape<LOG2N>::THREADS, TcShape<LOG2N>::CTAS_
         twi[i] = E::pack(s0f, s1f);
     }
 
-    const float4 *__restrict__ ring4 = reinterpret_cast<const float4 *>(a.ring);
-    const float2 *__restrict__ ring2 = a.ring;
-    const int items = a.D * a.R;
-    const int npairs = (a.count + 1) >> 1;
-    const unsigned long long wlim = (unsigned long long)a.wait_limit_ns;
-    const int smask = a.S - 1;
     uint32_t phA = 0, phB = 0;
     bool pendA = false, pendB = false;  // a commit not yet waited for
     bool failed = false;
-    for (int w = blockIdx.x; w < items && !failed; w += gridDim.x) {
+    int *status = nullptr;  // batch: the status word of the item that timed out
+    // Work item w of one handle: trial w % D, block range w / D.  False
+    // after a timed-out wait.
+    // one handle: these stay fixed for the whole launch
+    const float4 *__restrict__ ring4_0 = reinterpret_cast<const float4 *>(a0.ring);
+    const int npairs_0 = (a0.count + 1) >> 1;
+    const unsigned long long wlim_0 = (unsigned long long)a0.wait_limit_ns;
+    const int smask_0 = a0.S - 1;
+    auto run_item = [&](const DedispArgs &a, const int w) -> bool {
+        const float4 *__restrict__ ring4 = MULTI ? reinterpret_cast<const float4 *>(a.ring) : ring4_0;
+        const float2 *__restrict__ ring2 = reinterpret_cast<const float2 *>(ring4);
+        const int npairs = MULTI ? (a.count + 1) >> 1 : npairs_0;
+        const unsigned long long wlim = MULTI ? (unsigned long long)a.wait_limit_ns : wlim_0;
+        const int smask = MULTI ? a.S - 1 : smask_0;
+        if constexpr (MULTI) {
+            status = a.status;
+            if constexpr (FOLD)
+                fold_smem_layout(fw, sm + S::SMEM_FOLD, a.fold);
+        }
         const int dm = w % a.D;
         const int rr = w / a.D;
         const int kb = 2 * (int)((long long)npairs * rr / a.R);
@@ -654,7 +666,7 @@ __global__ void __launch_bounds__(TcShape<LOG2N>::THREADS, TcShape<LOG2N>::CTAS_
             }
         }
         if (failed)
-            break;
+            return false;
         if constexpr (FOLD) {
             __syncthreads();
             if (a.fold.smem_prof) {
@@ -667,9 +679,52 @@ __global__ void __launch_bounds__(TcShape<LOG2N>::THREADS, TcShape<LOG2N>::CTAS_
             }
             __syncthreads();
         }
+        return true;
+    };
+
+    if constexpr (!MULTI) {
+        const int items = a0.D * a0.R;
+        for (int w = blockIdx.x; w < items && !failed; w += gridDim.x)
+            run_item(a0, w);
+    } else {
+        // items of every handle of the batch, taken from a counter; the
+        // item's arguments are copied into shared memory
+        __shared__ DedispArgs sargs;
+        __shared__ int swork[2];
+        while (!failed) {
+            __syncthreads();  // every reader of sargs / swork is done
+            if (tid == 0) {
+                const int gw = atomicAdd(bt.counter, 1);
+                int o = -1;
+                if (gw < __ldg(bt.prefix + bt.nobs)) {
+                    int lo = 0, hi = bt.nobs - 1;  // last o with prefix[o] <= gw
+                    while (lo < hi) {
+                        const int mid = (lo + hi + 1) >> 1;
+                        if (__ldg(bt.prefix + mid) <= gw)
+                            lo = mid;
+                        else
+                            hi = mid - 1;
+                    }
+                    o = lo;
+                }
+                swork[0] = gw;
+                swork[1] = o;
+            }
+            __syncthreads();
+            const int gw = swork[0], o = swork[1];
+            if (o < 0)
+                break;
+            static_assert(sizeof(DedispArgs) % 4 == 0, "DedispArgs copied as words");
+            const uint32_t *src = reinterpret_cast<const uint32_t *>(bt.args + o);
+            uint32_t *dst = reinterpret_cast<uint32_t *>(&sargs);
+            for (int i = tid; i < (int)(sizeof(DedispArgs) / 4); i += T)
+                dst[i] = src[i];
+            __syncthreads();
+            run_item(sargs, gw - __ldg(bt.prefix + o));
+        }
     }
     if (failed && tid == 0) {
-        atomicExch(a.status, 1);
+        atomicExch(MULTI ? status : a0.status, 1);
         // the GEMMs still outstanding get the same time to finish
         if (pendA)
             mbar_wait(barA, phA, kWaitLimitNs);
@@ -738,25 +793,25 @@ __global__ void tc_permute_kernel(const float2 *__restrict__ in, float2 *__restr
         out[(i & ~nmask) + tc_pos((int)(i & nmask), log2n)] = in[i];
 }
 
-template <int LOG2N, class E, bool SERIES, bool FOLD>
-auto tc_fn() { return tc_dedisp_kernel<LOG2N, E, SERIES, FOLD>; }
+template <int LOG2N, class E, bool SERIES, bool FOLD, bool MULTI>
+auto tc_fn() { return tc_dedisp_kernel<LOG2N, E, SERIES, FOLD, MULTI>; }
 
-template <int LOG2N, class E, typename G>
+template <int LOG2N, class E, bool MULTI, typename G>
 auto tc_select_e(bool series, bool fold, G &&go)
 {
     if (series && fold)
-        return go(tc_fn<LOG2N, E, true, true>());
+        return go(tc_fn<LOG2N, E, true, true, MULTI>());
     if (fold)
-        return go(tc_fn<LOG2N, E, false, true>());
-    return go(tc_fn<LOG2N, E, true, false>());
+        return go(tc_fn<LOG2N, E, false, true, MULTI>());
+    return go(tc_fn<LOG2N, E, true, false, MULTI>());
 }
 
-template <int LOG2N, typename G>
+template <int LOG2N, bool MULTI = false, typename G>
 auto tc_select_n(bool bf16, bool series, bool fold, G &&go)
 {
     if (bf16)
-        return tc_select_e<LOG2N, BF16>(series, fold, go);
-    return tc_select_e<LOG2N, F16>(series, fold, go);
+        return tc_select_e<LOG2N, BF16, MULTI>(series, fold, go);
+    return tc_select_e<LOG2N, F16, MULTI>(series, fold, go);
 }
 
 template <int LOG2N>
@@ -784,25 +839,25 @@ int tc_blocks_per_sm_t(bool bf16, bool series, bool fold, size_t extra_smem)
     });
 }
 
-template <int LOG2N>
-cudaError_t launch_tc_t(bool bf16, bool series, bool fold, const DedispArgs &a, int grid, cudaStream_t st)
+template <int LOG2N, bool MULTI>
+cudaError_t launch_tc_t(bool bf16, bool series, bool fold, const DedispArgs &a, const BatchArgs &b,
+                        size_t fold_smem, int grid, cudaStream_t st)
 {
     using S = TcShape<LOG2N>;
-    const size_t sm = (size_t)S::SMEM_FOLD +
-                      (fold ? fold_smem_bytes(a.fold.nbins, a.fold.span_cap, a.fold.smem_prof != 0, S::THREADS) : 0);
+    const size_t sm = (size_t)S::SMEM_FOLD + (fold ? fold_smem : 0);
     // no more CTAs per SM than the tensor memory holds (shared memory decides)
     if (S::CTAS_PER_SM == 2 && sm * 3 <= 228u * 1024u)
         return cudaErrorInvalidConfiguration;
     if (S::CTAS_PER_SM == 1 && sm * 2 <= 228u * 1024u)
         return cudaErrorInvalidConfiguration;
-    return tc_select_n<LOG2N>(bf16, series, fold, [&](auto k) -> cudaError_t {
+    return tc_select_n<LOG2N, MULTI>(bf16, series, fold, [&](auto k) -> cudaError_t {
         cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e == cudaSuccess)
             e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout,
                                      (int)cudaSharedmemCarveoutMaxShared);
         if (e != cudaSuccess)
             return e;
-        k<<<grid, S::THREADS, sm, st>>>(a);
+        k<<<grid, S::THREADS, sm, st>>>(a, b);
         return cudaGetLastError();
     });
 }
@@ -829,9 +884,23 @@ cudaError_t launch_tc_dedisp(int log2n, bool bf16, bool series, bool fold, const
 {
     if (!a.status || !tc_supported(log2n))
         return cudaErrorInvalidValue;
+    const BatchArgs none{};
+    const size_t fs = fold ? fold_smem_bytes(a.fold.nbins, a.fold.span_cap, a.fold.smem_prof != 0, tc_threads(log2n))
+                           : 0;
     if (log2n == 13)
-        return launch_tc_t<13>(bf16, series, fold, a, grid, st);
-    return launch_tc_t<12>(bf16, series, fold, a, grid, st);
+        return launch_tc_t<13, false>(bf16, series, fold, a, none, fs, grid, st);
+    return launch_tc_t<12, false>(bf16, series, fold, a, none, fs, grid, st);
+}
+
+cudaError_t launch_tc_dedisp_batch(int log2n, bool bf16, bool series, bool fold, const BatchArgs &b,
+                                   size_t fold_smem, int grid, cudaStream_t st)
+{
+    if (!b.args || !b.prefix || !b.counter || b.nobs < 1 || !tc_supported(log2n))
+        return cudaErrorInvalidValue;
+    DedispArgs none{};
+    if (log2n == 13)
+        return launch_tc_t<13, true>(bf16, series, fold, none, b, fold_smem, grid, st);
+    return launch_tc_t<12, true>(bf16, series, fold, none, b, fold_smem, grid, st);
 }
 
 cudaError_t launch_tc_permute_rows(const float2 *in, float2 *out, int rows, int log2n, cudaStream_t st)

@@ -203,6 +203,12 @@ class Dedisperser:
     def synchronize(self) -> None:
         check(lib().msosm_dedisp_synchronize(self._h))
 
+    def reset(self) -> None:
+        """Start a new input stream (same band and trials): the history is
+        forgotten and folding unconfigured (call fold_init again)."""
+        check(lib().msosm_dedisp_reset(self._h))
+        self.folding = False
+
     def enable_timing(self, on: bool = True) -> None:
         """Record CUDA events around each stage of every filter call."""
         check(lib().msosm_dedisp_enable_timing(self._h, int(on)))
@@ -215,6 +221,69 @@ class Dedisperser:
     def close(self) -> None:
         if getattr(self, "_h", None) is not None and self._h.value:
             lib().msosm_dedisp_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class DedispBatch:
+    """One filter call of many Dedisperser handles (observations of any
+    length, band and trial grid) with one persistent launch per group of
+    handles that run the same tensor-core kernel (msosm_batch): work items
+    of every observation are handed out largest first from a counter.
+    Handles of other kernels run their calls one after another inside the
+    same call.  While in a batch the handles run on the batch's stream;
+    read their results with their own get_output / get_profiles."""
+
+    def __init__(self, dedispersers: Sequence[Dedisperser]):
+        self.members = list(dedispersers)
+        arr = (ctypes.c_void_p * len(self.members))(*[d._h.value for d in self.members])
+        h = ctypes.c_void_p()
+        check(lib().msosm_batch_create(arr, len(self.members), ctypes.byref(h)))
+        self._h = h
+
+    def info(self) -> dict:
+        g, l, it = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check(lib().msosm_batch_get_info(self._h, ctypes.byref(g), ctypes.byref(l), ctypes.byref(it)))
+        return {"groups": g.value, "launches_per_call": l.value, "items": it.value}
+
+    def filter_block(self, inputs) -> None:
+        """inputs[i]: the next count*M samples of member i (host arrays or
+        CUDA tensors, all complex64 or all uint16 pairs)."""
+        if len(inputs) != len(self.members):
+            raise ValueError("one input per member")
+        ptrs, kinds, keep = [], set(), []
+        for d, x in zip(self.members, inputs):
+            p, kind, k = _input_pointer(x, d.block_samples)
+            ptrs.append(p)
+            kinds.add(kind)
+            keep.append(k)
+            if not isinstance(k, np.ndarray):
+                import torch
+                torch.cuda.current_stream(k.device).synchronize()
+        if len(kinds) != 1:
+            raise ValueError("all inputs of a batch call must be of one kind")
+        arr = (ctypes.c_void_p * len(ptrs))(*ptrs)
+        kind = _abi.INPUT_C64 if kinds.pop() == "c64" else _abi.INPUT_UINT16
+        check(lib().msosm_batch_filter(self._h, arr, kind))
+        del keep
+
+    def set_stream(self, stream) -> None:
+        """Run on a CUDA stream (torch.cuda.Stream or a raw cudaStream_t);
+        None returns to the batch's own stream."""
+        ptr = getattr(stream, "cuda_stream", stream) or 0
+        check(lib().msosm_batch_set_stream(self._h, ctypes.c_void_p(ptr)))
+
+    def synchronize(self) -> None:
+        check(lib().msosm_batch_synchronize(self._h))
+
+    def close(self) -> None:
+        if getattr(self, "_h", None) is not None and self._h.value:
+            lib().msosm_batch_destroy(self._h)
             self._h = ctypes.c_void_p()
 
     def __del__(self):

@@ -133,23 +133,46 @@ def normalise(prof: np.ndarray) -> np.ndarray:
     return (x / s if s > 0 else x).astype(np.float32)
 
 
+_HANDLES: "dict" = {}   # trial grid -> Dedisperser, most recently used last
+_HANDLE_CACHE = 9  # the coarse grid, the sweep's chunks and the windows of one observation
+
+
+def _handle(band: Band, dms: np.ndarray):
+    """A dedisperser for this band and trial grid, reset for a new stream:
+    kept across observations (the filters and ring of a grid are designed
+    and allocated once), at most _HANDLE_CACHE grids."""
+    from .dedisp import Dedisperser
+    key = (band.bw, band.f0, band.fftpoint, band.samples, band.precision, dms.tobytes())
+    d = _HANDLES.pop(key, None)
+    if d is None:
+        while len(_HANDLES) >= _HANDLE_CACHE:
+            _HANDLES.pop(next(iter(_HANDLES))).close()
+        d = Dedisperser(band.bw, dms, band.f0, band.fftpoint, count=band.samples // (band.fftpoint // 2),
+                        series=False, precision=band.precision)
+    else:
+        d.reset()
+    _HANDLES[key] = d
+    return d
+
+
+def release_handles() -> None:
+    """Free the dedispersers kept by fold_trials."""
+    while _HANDLES:
+        _HANDLES.pop(next(iter(_HANDLES))).close()
+
+
 def fold_trials(x, band: Band, dms: Sequence[float], period: float, nbins: Optional[int] = None) -> np.ndarray:
     """Folded |y|^2 profiles [len(dms), nbins] of one observation (device
     tensor of band.samples complex64) at the given trials."""
-    from .dedisp import Dedisperser
     M = band.fftpoint // 2
     nb = nbins or band.nbins
     ps = int(np.float32(period) * np.float32(band.bw))
     nb = min(nb, ps)
-    d = Dedisperser(band.bw, np.asarray(dms, np.float32), band.f0, band.fftpoint, count=band.samples // M,
-                    series=False, precision=band.precision)
-    try:
-        info = d.info()
-        d.fold_init(period, band.bw, time_bin=nb, discard_Nd=int(info.max_delaycount) * M, detect="power")
-        d.filter_block(x)
-        return d.get_profiles()
-    finally:
-        d.close()
+    d = _handle(band, np.ascontiguousarray(np.asarray(dms, np.float32)))
+    info = d.info()
+    d.fold_init(period, band.bw, time_bin=nb, discard_Nd=int(info.max_delaycount) * M, detect="power")
+    d.filter_block(x)
+    return d.get_profiles()
 
 
 def draw_pulsar(rng, band: Band, dm_range=None, period=(1e-3, 1.0), duty=(0.01, 0.10), snr=(0.01, 0.2)):
@@ -177,7 +200,12 @@ def simulate_profiles(n: int, band: Band, seed: int = 0, noise_fraction: float =
     meta = []
     step = band.dm_max / (band.coarse - 1)
     dev = torch.device("cuda")
+    import sys
+    import time
+    t0 = time.time()
     for i in range(n):
+        if i and i % 2000 == 0:
+            print(f"simulate_profiles: {i}/{n} in {time.time() - t0:.0f} s", file=sys.stderr, flush=True)
         p = draw_pulsar(rng, band, **ranges)
         pulsar = rng.random() >= noise_fraction
         x = pulsar_baseband(band.samples, band.bw, band.f0, p["dm"], p["period"], p["duty"],

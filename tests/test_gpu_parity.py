@@ -244,3 +244,25 @@ def test_bad_arguments_raise():
         d.filter_block(noise(100, 0))
     with pytest.raises(MsosmError):
         d.fold_init(0.001, BW, time_bin=10 ** 6)
+
+
+@pytest.mark.parametrize("precision", ["fp32", "fp16"])
+def test_reset_starts_a_new_stream_like_a_fresh_handle(precision):
+    # stream A for three calls, reset, stream B with a new fold period: the
+    # series and profiles equal a fresh handle's on stream B
+    dms = [0.0, 20.0, 55.0]
+    d = Dedisperser(BW, dms, F0, 4096, 6, precision=precision)
+    d.fold_init(0.00031, BW, time_bin=32, discard_Nd=int(d.Nd.max()), detect="power")
+    for c in range(3):
+        d.filter_block(noise(d.block_samples, 100 + c))
+    d.reset()
+    d.fold_init(0.00047, BW, time_bin=48, discard_Nd=int(d.Nd.max()), detect="power")
+    f = Dedisperser(BW, dms, F0, 4096, 6, precision=precision)
+    f.fold_init(0.00047, BW, time_bin=48, discard_Nd=int(f.Nd.max()), detect="power")
+    for c in range(4):
+        x = noise(d.block_samples, 200 + c)
+        d.filter_block(x)
+        f.filter_block(x)
+        np.testing.assert_array_equal(d.get_output(), f.get_output())
+    np.testing.assert_array_equal(d.get_profiles(), f.get_profiles())
+    assert d.folded_periods() == f.folded_periods() > 0
