@@ -573,16 +573,18 @@ __global__ void __launch_bounds__(TcShape<LOG2N>::THREADS, TcShape<LOG2N>::CTAS_
                 }
             }
             if constexpr (FOLD) {
+                // detected in the item's scale; its partial profiles are
+                // rescaled once at the end of the item (the scale is a power
+                // of two, fixed for the item)
                 float *ib = reinterpret_cast<float *>(op) + ob * M + 16 * N2 * oh + om2;
-                const float is2 = isc * isc;
                 if (a.fold.detect) {
 #pragma unroll
                     for (int u = 0; u < 16; ++u)
-                        ib[N2 * u] = sqrtf((yr[u] * yr[u] + yi[u] * yi[u]) * is2);
+                        ib[N2 * u] = sqrtf(yr[u] * yr[u] + yi[u] * yi[u]);
                 } else {
 #pragma unroll
                     for (int u = 0; u < 16; ++u)
-                        ib[N2 * u] = (yr[u] * yr[u] + yi[u] * yi[u]) * is2;
+                        ib[N2 * u] = yr[u] * yr[u] + yi[u] * yi[u];
                 }
             }
         };
@@ -669,12 +671,20 @@ __global__ void __launch_bounds__(TcShape<LOG2N>::THREADS, TcShape<LOG2N>::CTAS_
             return false;
         if constexpr (FOLD) {
             __syncthreads();
+            // the item's intensities were folded in its scale: |y|^2 carries
+            // sc^2 (|y| carries sc); undo it on the item's partial rows
+            const float back = a.fold.detect ? isc : isc * isc;
+            float *gm = a.fold.part_main + (size_t)w * a.fold.nbins;
+            float *gp = a.fold.part_pend + (size_t)w * a.fold.nbins;
             if (a.fold.smem_prof) {
-                float *gm = a.fold.part_main + (size_t)w * a.fold.nbins;
-                float *gp = a.fold.part_pend + (size_t)w * a.fold.nbins;
                 for (int i = tid; i < a.fold.nbins; i += blockDim.x) {
-                    gm[i] = fw.prof_main[i];
-                    gp[i] = fw.prof_pend[i];
+                    gm[i] = fw.prof_main[i] * back;
+                    gp[i] = fw.prof_pend[i] * back;
+                }
+            } else {
+                for (int i = tid; i < a.fold.nbins; i += blockDim.x) {
+                    gm[i] *= back;
+                    gp[i] *= back;
                 }
             }
             __syncthreads();
