@@ -78,14 +78,22 @@ __device__ __forceinline__ int div_bpt(int x, int bpt, float inv_bpt)
     return q;
 }
 
-// ibuf holds intensities at index t + t/32 (one pad slot per 32 samples), so
-// that threads reading bins of any length hit different banks
+// Layouts of the intensity buffer (sample t of the buffer at index ...):
+//  kIbufPadded: t + t/32, one pad slot per 32 samples, so that threads
+//    reading bins of any length one sample at a time hit different banks;
+//  kIbufSwizzled: t with its 16-byte chunk index c = t/4 XORed with
+//    (c/8) % 4: eight threads reading 16 (or 8) consecutive samples each as
+//    128-bit loads touch eight different 16-byte bank groups (plain, every
+//    second thread would meet the same group), and a warp storing 32
+//    consecutive samples still fills one 128-byte row.  The swizzle moves
+//    chunks only inside aligned 32-sample groups.
+constexpr int kIbufPadded = 1, kIbufSwizzled = 2;
 __device__ __forceinline__ int ipad(int t) { return t + (t >> 5); }
-// the intensity buffer index of sample t: padded (PAD) or plain
-template <bool PAD>
-__device__ __forceinline__ int iidx(int t) { return PAD ? ipad(t) : t; }
+__device__ __forceinline__ int iswz(int t) { return t ^ (((t >> 5) & 3) << 2); }
+template <int L>
+__device__ __forceinline__ int iidx(int t) { return L == kIbufPadded ? ipad(t) : iswz(t); }
 
-template <bool PAD>
+template <int L>
 __device__ __forceinline__ void fold_piece(const FoldArgs &f, float *prof, const float *ibuf, int off,
                                            int ph_lo, int ph_hi)
 {
@@ -113,11 +121,11 @@ __device__ __forceinline__ void fold_piece(const FoldArgs &f, float *prof, const
             const int s_hi = min(ph_hi, s0 + f.bpt);
             int p = s_lo + l;
             for (; p + G < s_hi; p += 2 * G) {
-                a0 += ibuf[iidx<PAD>(off + p)];
-                a1 += ibuf[iidx<PAD>(off + p + G)];
+                a0 += ibuf[iidx<L>(off + p)];
+                a1 += ibuf[iidx<L>(off + p + G)];
             }
             if (p < s_hi)
-                a0 += ibuf[iidx<PAD>(off + p)];
+                a0 += ibuf[iidx<L>(off + p)];
         }
         float sum = a0 + a1;
         for (int o = G >> 1; o > 0; o >>= 1)
@@ -135,11 +143,11 @@ __device__ __forceinline__ void fold_piece(const FoldArgs &f, float *prof, const
 // is then completed by the thread holding its first sample (thread 0 for the
 // bin running into the range), adding the following threads' first-bin sums
 // in thread order.
-template <bool PAD, int SPT = 8>
+template <int L, int SPT = 8>
 __device__ __forceinline__ void fold_block_fast(const FoldArgs &f, FoldSmem &w, float *prof, const float *ibuf,
                                                 int ph_lo, int n_valid)
 {
-    static_assert(SPT == 8 || (SPT == 16 && !PAD), "8 samples per thread, or 16 from a plain buffer");
+    static_assert(SPT == 8 || (SPT == 16 && L == kIbufSwizzled), "8 samples per thread, or 16 from a swizzled buffer");
     const int tid = threadIdx.x, T = blockDim.x;
     const int bpt = f.bpt;
     const int j0 = SPT * tid;
@@ -149,14 +157,16 @@ __device__ __forceinline__ void fold_block_fast(const FoldArgs &f, FoldSmem &w, 
     const int n0 = bpt - r0;       // samples left in bin b0 (>= 1)
     const int nv = min(SPT, n_valid - j0);
     float x[SPT];
-    if constexpr (PAD) {
+    if constexpr (L == kIbufPadded) {
 #pragma unroll
         for (int u = 0; u < SPT; ++u)
             x[u] = ibuf[ipad(j0 + u)];
     } else {
+        // chunks c = (SPT/4) tid + v, stored at c ^ ((c / 8) % 4)
+        const int sw = ((SPT / 4) * tid >> 3) & 3;
 #pragma unroll
         for (int v = 0; v < SPT / 4; ++v) {
-            const float4 q = reinterpret_cast<const float4 *>(ibuf)[(SPT / 4) * tid + v];
+            const float4 q = reinterpret_cast<const float4 *>(ibuf)[((SPT / 4) * tid + v) ^ sw];
             x[4 * v] = q.x;
             x[4 * v + 1] = q.y;
             x[4 * v + 2] = q.z;
@@ -223,6 +233,7 @@ __device__ __forceinline__ void fold_block_fast(const FoldArgs &f, FoldSmem &w, 
 // 8 * blockDim.x) in one pass of 16 samples per thread, when one span covers
 // them and bins hold >= 16 samples; false (nothing folded) when the caller
 // has to fold them block by block.
+template <int L>
 __device__ __forceinline__ bool fold_pair(const FoldArgs &f, FoldSmem &w, const float *ibuf, int t0, int M, int &sp,
                                           int &base, int &cnt)
 {
@@ -247,14 +258,14 @@ __device__ __forceinline__ bool fold_pair(const FoldArgs &f, FoldSmem &w, const 
         const int ph_lo = w.wp[i] + (t0 - sa);
         const int n_valid = min(2 * M, f.nbins * f.bpt - ph_lo);
         if (n_valid > 0)
-            fold_block_fast<false, 16>(f, w, dest == 1 ? w.prof_main : w.prof_pend, ibuf, ph_lo, n_valid);
+            fold_block_fast<L, 16>(f, w, dest == 1 ? w.prof_main : w.prof_pend, ibuf, ph_lo, n_valid);
     }
     return true;
 }
 
 // Fold the M intensities of one block (ibuf: chunk-local samples t0..t0+M-1).
 // sp/base/cnt: the work item's running span cursor and window (uniform).
-template <bool PAD>
+template <int L>
 __device__ __forceinline__ void fold_block(const FoldArgs &f, FoldSmem &w, const float *ibuf, int t0, int M,
                                            int &sp, int &base, int &cnt)
 {
@@ -276,7 +287,7 @@ __device__ __forceinline__ void fold_block(const FoldArgs &f, FoldSmem &w, const
                 const int ph_lo = w.wp[i] + (t0 - sa);
                 const int n_valid = min(M, f.nbins * f.bpt - ph_lo);
                 if (n_valid > 0)
-                    fold_block_fast<PAD>(f, w, dest == 1 ? w.prof_main : w.prof_pend, ibuf, ph_lo, n_valid);
+                    fold_block_fast<L>(f, w, dest == 1 ? w.prof_main : w.prof_pend, ibuf, ph_lo, n_valid);
             }
             return;
         }
@@ -295,7 +306,7 @@ __device__ __forceinline__ void fold_block(const FoldArgs &f, FoldSmem &w, const
             const int a = max(sa, t0), b = min(sb, t1);
             if (a < b) {
                 const int ph_lo = w.wp[i] + (a - sa);
-                fold_piece<PAD>(f, dest == 1 ? w.prof_main : w.prof_pend, ibuf, a - t0 - ph_lo, ph_lo, ph_lo + (b - a));
+                fold_piece<L>(f, dest == 1 ? w.prof_main : w.prof_pend, ibuf, a - t0 - ph_lo, ph_lo, ph_lo + (b - a));
             }
             // a later span of this block may fold into the same bins
             if (sb < t1)

@@ -195,7 +195,7 @@ __global__ void __launch_bounds__(FftShape<LOG2N>::T) dedisp_kernel(DedispArgs a
             }
             if constexpr (FOLD) {
                 __syncthreads();
-                fold_block<true>(a.fold, fw, ibuf, k * M, M, sp, sbase, scnt);
+                fold_block<kIbufPadded>(a.fold, fw, ibuf, k * M, M, sp, sbase, scnt);
             }
         }
         if constexpr (FOLD) {
@@ -264,7 +264,7 @@ __global__ void __launch_bounds__(256) fold_series_kernel(const float *__restric
             for (int t = threadIdx.x; t < kFoldBlock; t += blockDim.x)
                 ibuf[ipad(t)] = (long long)t0 + t < n ? I[t0 + t] : 0.f;
             __syncthreads();
-            fold_block<true>(f, fw, ibuf, t0, kFoldBlock, sp, sbase, scnt);
+            fold_block<kIbufPadded>(f, fw, ibuf, t0, kFoldBlock, sp, sbase, scnt);
             __syncthreads();
         }
         if (f.smem_prof) {

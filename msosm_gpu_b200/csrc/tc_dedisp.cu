@@ -576,15 +576,20 @@ __global__ void __launch_bounds__(TcShape<LOG2N>::THREADS, TcShape<LOG2N>::CTAS_
                 // detected in the item's scale; its partial profiles are
                 // rescaled once at the end of the item (the scale is a power
                 // of two, fixed for the item)
-                float *ib = reinterpret_cast<float *>(op) + ob * M + 16 * N2 * oh + om2;
+                // sample t = t0 + N2 u at iswz(t) (kIbufSwizzled): adding
+                // N2 u = 128 u leaves the swizzle bits alone; adding 64 u
+                // flips their upper bit with u's parity
+                float *ib = reinterpret_cast<float *>(op);
+                const int t0 = ob * M + 16 * N2 * oh + om2;
+                const int e0 = iswz(t0), e1 = N2 == 64 ? iswz(t0 + 64) - 64 : e0;
                 if (a.fold.detect) {
 #pragma unroll
                     for (int u = 0; u < 16; ++u)
-                        ib[N2 * u] = sqrtf(yr[u] * yr[u] + yi[u] * yi[u]);
+                        ib[((u & 1) ? e1 : e0) + N2 * u] = sqrtf(yr[u] * yr[u] + yi[u] * yi[u]);
                 } else {
 #pragma unroll
                     for (int u = 0; u < 16; ++u)
-                        ib[N2 * u] = yr[u] * yr[u] + yi[u] * yi[u];
+                        ib[((u & 1) ? e1 : e0) + N2 * u] = yr[u] * yr[u] + yi[u] * yi[u];
                 }
             }
         };
@@ -641,11 +646,11 @@ __global__ void __launch_bounds__(TcShape<LOG2N>::THREADS, TcShape<LOG2N>::CTAS_
                     const int k = kb + 2 * i;
                     const float *ib0 = reinterpret_cast<const float *>(sm + cur);
                     __syncthreads();
-                    if (!(k + 1 < ke && fold_pair(a.fold, fw, ib0, k * M, M, sp, sbase, scnt))) {
-                        fold_block<false>(a.fold, fw, ib0, k * M, M, sp, sbase, scnt);
+                    if (!(k + 1 < ke && fold_pair<kIbufSwizzled>(a.fold, fw, ib0, k * M, M, sp, sbase, scnt))) {
+                        fold_block<kIbufSwizzled>(a.fold, fw, ib0, k * M, M, sp, sbase, scnt);
                         if (k + 1 < ke) {
                             __syncthreads();
-                            fold_block<false>(a.fold, fw, ib0 + M, (k + 1) * M, M, sp, sbase, scnt);
+                            fold_block<kIbufSwizzled>(a.fold, fw, ib0 + M, (k + 1) * M, M, sp, sbase, scnt);
                         }
                     }
                 }
