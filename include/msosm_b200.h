@@ -542,7 +542,7 @@ MSOSM_API msosm_status msosm_cnn_adam_step(msosm_cnn *n, float lr);
 
 /* Limit of each wait of the tensor-core kernel (MSOSM_FLAG_TENSOR_*) on one
  * of its GEMMs, in ns of the global timer; ns < 0 restores the default (1 s),
- * 0 gives up at the first probe that finds a GEMM unfinished.  When a wait
+ * 0 makes every such wait give up at once.  When a wait
  * gives up, the kernel records a nonzero status, waits (1 s at most) for the
  * GEMMs it still has in flight, frees its tensor memory and returns; the
  * next synchronising call (get_output_*, get_profiles, synchronize) returns

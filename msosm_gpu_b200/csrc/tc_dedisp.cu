@@ -91,16 +91,17 @@ __device__ __forceinline__ bool mbar_test_wait(uint32_t bar, uint32_t parity)
 }
 
 // Waits for the phase of the given parity to complete; false after limit_ns.
-// A limit below the suspend hint probes without suspending, and a limit of
-// 0 gives up at the first probe that finds the phase incomplete (a
-// diagnostic setting: the kernel then takes its timeout exit).
+// A limit below the suspend hint probes without suspending; a limit of 0
+// gives up at once, without probing (a diagnostic setting: the kernel then
+// takes its timeout exit, whose drain of the GEMMs in flight keeps its own
+// limit).
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, unsigned long long limit_ns)
 {
+    if (limit_ns == 0)
+        return false;
     if (limit_ns < kSuspendHintNs) {
         if (mbar_test_wait(bar, parity))
             return true;
-        if (limit_ns == 0)
-            return false;
         const unsigned long long t0 = global_ns();
         while (!mbar_test_wait(bar, parity))
             if (global_ns() - t0 > limit_ns)
@@ -340,7 +341,7 @@ __device__ __forceinline__ void pow2_scale_to(float mx, float &s, float &inv)
 
 template <int LOG2N, class E, bool SERIES, bool FOLD, bool MULTI>
 __global__ void __launch_bounds__(TcShape<LOG2N>::THREADS, TcShape<LOG2N>::CTAS_PER_SM)
-    tc_dedisp_kernel(DedispArgs a0, BatchArgs bt)
+    tc_dedisp_kernel(const __grid_constant__ DedispArgs a0, const __grid_constant__ BatchArgs bt)
 {
     using S = TcShape<LOG2N>;
     constexpr int N = S::N, M = S::M, N2 = S::N2, W = S::WARPS, T = S::THREADS;
@@ -384,22 +385,61 @@ __global__ void __launch_bounds__(TcShape<LOG2N>::THREADS, TcShape<LOG2N>::CTAS_
     int *status = nullptr;  // batch: the status word of the item that timed out
     // Work item w of one handle: trial w % D, block range w / D.  False
     // after a timed-out wait.
-    // one handle: these stay fixed for the whole launch
-    const float4 *__restrict__ ring4_0 = reinterpret_cast<const float4 *>(a0.ring);
-    const int npairs_0 = (a0.count + 1) >> 1;
-    const unsigned long long wlim_0 = (unsigned long long)a0.wait_limit_ns;
-    const int smask_0 = a0.S - 1;
-    auto run_item = [&](const DedispArgs &a, const int w) -> bool {
-        const float4 *__restrict__ ring4 = MULTI ? reinterpret_cast<const float4 *>(a.ring) : ring4_0;
-        const float2 *__restrict__ ring2 = reinterpret_cast<const float2 *>(ring4);
-        const int npairs = MULTI ? (a.count + 1) >> 1 : npairs_0;
-        const unsigned long long wlim = MULTI ? (unsigned long long)a.wait_limit_ns : wlim_0;
-        const int smask = MULTI ? a.S - 1 : smask_0;
+    // Work items: with one handle, trial w % D, block range w / D of a0, w
+    // strided over the grid; in a batch, the next item of any handle from the
+    // counter, its arguments copied into shared memory.  The item body is
+    // written once, inside the loop (as a lambda it cost registers and time).
+    __shared__ DedispArgs sargs;  // batch only
+    __shared__ int swork[2];
+    const int items0 = MULTI ? 0 : a0.D * a0.R;
+    for (int it = 0; !failed; ++it) {
+        int w;
+        if constexpr (!MULTI) {
+            w = blockIdx.x + it * gridDim.x;
+            if (w >= items0)
+                break;
+        } else {
+            __syncthreads();  // every reader of sargs / swork is done
+            if (tid == 0) {
+                const int gw = atomicAdd(bt.counter, 1);
+                int o = -1;
+                if (gw < __ldg(bt.prefix + bt.nobs)) {
+                    int lo = 0, hi = bt.nobs - 1;  // last o with prefix[o] <= gw
+                    while (lo < hi) {
+                        const int mid = (lo + hi + 1) >> 1;
+                        if (__ldg(bt.prefix + mid) <= gw)
+                            lo = mid;
+                        else
+                            hi = mid - 1;
+                    }
+                    o = lo;
+                }
+                swork[0] = o < 0 ? -1 : gw - __ldg(bt.prefix + o);
+                swork[1] = o;
+            }
+            __syncthreads();
+            const int o = swork[1];
+            if (o < 0)
+                break;
+            w = swork[0];
+            static_assert(sizeof(DedispArgs) % 4 == 0, "DedispArgs copied as words");
+            const uint32_t *src = reinterpret_cast<const uint32_t *>(bt.args + o);
+            uint32_t *dst = reinterpret_cast<uint32_t *>(&sargs);
+            for (int i = tid; i < (int)(sizeof(DedispArgs) / 4); i += T)
+                dst[i] = src[i];
+            __syncthreads();
+        }
+        const DedispArgs &a = MULTI ? sargs : a0;
         if constexpr (MULTI) {
             status = a.status;
             if constexpr (FOLD)
                 fold_smem_layout(fw, sm + S::SMEM_FOLD, a.fold);
         }
+        const float4 *__restrict__ ring4 = reinterpret_cast<const float4 *>(a.ring);
+        const float2 *__restrict__ ring2 = a.ring;
+        const int npairs = (a.count + 1) >> 1;
+        const unsigned long long wlim = (unsigned long long)a.wait_limit_ns;
+        const int smask = a.S - 1;
         const int dm = w % a.D;
         const int rr = w / a.D;
         const int kb = 2 * (int)((long long)npairs * rr / a.R);
@@ -673,7 +713,7 @@ __global__ void __launch_bounds__(TcShape<LOG2N>::THREADS, TcShape<LOG2N>::CTAS_
             }
         }
         if (failed)
-            return false;
+            break;
         if constexpr (FOLD) {
             __syncthreads();
             // the item's intensities were folded in its scale: |y|^2 carries
@@ -693,49 +733,6 @@ __global__ void __launch_bounds__(TcShape<LOG2N>::THREADS, TcShape<LOG2N>::CTAS_
                 }
             }
             __syncthreads();
-        }
-        return true;
-    };
-
-    if constexpr (!MULTI) {
-        const int items = a0.D * a0.R;
-        for (int w = blockIdx.x; w < items && !failed; w += gridDim.x)
-            run_item(a0, w);
-    } else {
-        // items of every handle of the batch, taken from a counter; the
-        // item's arguments are copied into shared memory
-        __shared__ DedispArgs sargs;
-        __shared__ int swork[2];
-        while (!failed) {
-            __syncthreads();  // every reader of sargs / swork is done
-            if (tid == 0) {
-                const int gw = atomicAdd(bt.counter, 1);
-                int o = -1;
-                if (gw < __ldg(bt.prefix + bt.nobs)) {
-                    int lo = 0, hi = bt.nobs - 1;  // last o with prefix[o] <= gw
-                    while (lo < hi) {
-                        const int mid = (lo + hi + 1) >> 1;
-                        if (__ldg(bt.prefix + mid) <= gw)
-                            lo = mid;
-                        else
-                            hi = mid - 1;
-                    }
-                    o = lo;
-                }
-                swork[0] = gw;
-                swork[1] = o;
-            }
-            __syncthreads();
-            const int gw = swork[0], o = swork[1];
-            if (o < 0)
-                break;
-            static_assert(sizeof(DedispArgs) % 4 == 0, "DedispArgs copied as words");
-            const uint32_t *src = reinterpret_cast<const uint32_t *>(bt.args + o);
-            uint32_t *dst = reinterpret_cast<uint32_t *>(&sargs);
-            for (int i = tid; i < (int)(sizeof(DedispArgs) / 4); i += T)
-                dst[i] = src[i];
-            __syncthreads();
-            run_item(sargs, gw - __ldg(bt.prefix + o));
         }
     }
     if (failed && tid == 0) {

@@ -141,8 +141,7 @@ class Dedisperser:
 
     def set_tc_wait_limit(self, ns: int) -> None:
         """Limit of each wait of the tensor-core kernel on a GEMM, in ns
-        (negative: the default 1 s; 0: give up at the first unfinished
-        probe).  A wait that gives up makes the next synchronising call raise
+        (negative: the default 1 s; 0: every wait gives up at once).  A wait that gives up makes the next synchronising call raise
         a timeout; the handle then carries on.  For tests of that path."""
         check(lib().msosm_dedisp_set_tc_wait_limit(self._h, int(ns)))
 

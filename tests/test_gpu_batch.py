@@ -14,10 +14,10 @@ pytestmark = pytest.mark.gpu
 
 SERIES_TOL, FOLD_TOL = 1.5e-3, 1e-4
 
-OBS = [  # bw, f0, dms, fftpoint, count, precision, period
-    (16e6, 1242e6, [0.0, 30.0, 73.2], 4096, 12, "fp16", 0.00031),
-    (64e6, 1368e6, [5.0, 40.0], 8192, 7, "fp16", 0.0007),
-    (32e6, 1384e6, [1.0, 12.0, 20.0, 25.0], 4096, 5, "fp16", 0.00045),
+OBS = [  # bw, f0, dms, fftpoint, count, precision, period (smears short enough to fold whole periods)
+    (16e6, 1242e6, [0.0, 3.0, 8.0], 4096, 12, "fp16", 0.00031),
+    (64e6, 1368e6, [0.5, 2.0], 8192, 7, "fp16", 0.0002),
+    (32e6, 1384e6, [1.0, 4.0, 6.0, 8.0], 4096, 12, "fp16", 0.00045),
     (16e6, 1242e6, [2.0, 9.0], 4096, 9, "fp16", 0.00029),
     (4e6, 1098e6, [3.0, 30.0], 2048, 6, "fp32", 0.0013),
 ]
@@ -36,7 +36,7 @@ def make(o, nbins=64):
 
 def test_batch_matches_oracle_and_own_handles():
     rng = np.random.default_rng(5)
-    calls = 3
+    calls = 4
     batch_h = [make(o) for o in OBS]
     solo_h = [make(o) for o in OBS]
     b = DedispBatch(batch_h)

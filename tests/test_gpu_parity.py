@@ -250,7 +250,9 @@ def test_bad_arguments_raise():
 def test_reset_starts_a_new_stream_like_a_fresh_handle(precision):
     # stream A for three calls, reset, stream B with a new fold period: the
     # series and profiles equal a fresh handle's on stream B
-    dms = [0.0, 20.0, 55.0]
+    # smears below two periods of 0.47 ms, so that the 4 calls of stream B
+    # fold whole periods
+    dms = [0.0, 5.0, 12.0]
     d = Dedisperser(BW, dms, F0, 4096, 6, precision=precision)
     d.fold_init(0.00031, BW, time_bin=32, discard_Nd=int(d.Nd.max()), detect="power")
     for c in range(3):
