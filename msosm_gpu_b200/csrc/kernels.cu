@@ -340,21 +340,41 @@ __global__ void __launch_bounds__(FftShape<LOG2N>::T) design_kernel(DesignArgs a
 // small kernels
 // ---------------------------------------------------------------------------
 
-__global__ void fold_reduce_kernel(const float *__restrict__ pm, const float *__restrict__ pp, int D, int R,
-                                   int nbins, double *am, double *ap)
+// Sum of the R partial rows of every (trial, bin), in double and in a fixed
+// order: G groups of rows (group g: rows g, g + G, ...) are summed by G
+// threads, then thread g = 0 adds the G group sums in group order.  A thread
+// block covers 32 consecutive (trial, bin) indices x G groups; row r of index
+// i sits at r * D * nbins + i, so a warp reads 128 contiguous bytes of a row.
+template <int G>
+__global__ void __launch_bounds__(32 * G) fold_reduce_kernel(const float *__restrict__ pm,
+                                                             const float *__restrict__ pp, int D, int R, int nbins,
+                                                             double *am, double *ap)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= D * nbins)
-        return;
-    const int dm = i / nbins, bin = i % nbins;
+    __shared__ double part[2][G][32];
+    const int lane = threadIdx.x & 31, g = threadIdx.x >> 5;
+    const long long n = (long long)D * nbins;
+    const long long i = (long long)blockIdx.x * 32 + lane;
     double sm = 0.0, sp = 0.0;
-    for (int r = 0; r < R; ++r) {
-        const size_t row = ((size_t)r * D + dm) * nbins + bin;
-        sm += (double)pm[row];
-        sp += (double)pp[row];
+    if (i < n) {
+        for (int r = g; r < R; r += G) {
+            const size_t row = (size_t)r * (size_t)n + (size_t)i;
+            sm += (double)pm[row];
+            sp += (double)pp[row];
+        }
     }
-    am[i] += sm;
-    ap[i] += sp;
+    part[0][g][lane] = sm;
+    part[1][g][lane] = sp;
+    __syncthreads();
+    if (g == 0 && i < n) {
+        double a = 0.0, b = 0.0;
+#pragma unroll
+        for (int k = 0; k < G; ++k) {
+            a += part[0][k][lane];
+            b += part[1][k][lane];
+        }
+        am[i] += a;
+        ap[i] += b;
+    }
 }
 
 __global__ void fold_flush_kernel(double *am, double *ap, size_t n)
@@ -564,7 +584,20 @@ cudaError_t launch_fold_reduce(const float *pm, const float *pp, int D, int R, i
                                double *ap, cudaStream_t st)
 {
     const size_t n = (size_t)D * nbins;
-    fold_reduce_kernel<<<blocks_for(n, 256), 256, 0, st>>>(pm, pp, D, R, nbins, am, ap);
+    const unsigned int blocks = blocks_for(n, 32);
+    // row groups: the largest power of two <= min(R, 32)
+    if (R >= 32)
+        fold_reduce_kernel<32><<<blocks, 32 * 32, 0, st>>>(pm, pp, D, R, nbins, am, ap);
+    else if (R >= 16)
+        fold_reduce_kernel<16><<<blocks, 32 * 16, 0, st>>>(pm, pp, D, R, nbins, am, ap);
+    else if (R >= 8)
+        fold_reduce_kernel<8><<<blocks, 32 * 8, 0, st>>>(pm, pp, D, R, nbins, am, ap);
+    else if (R >= 4)
+        fold_reduce_kernel<4><<<blocks, 32 * 4, 0, st>>>(pm, pp, D, R, nbins, am, ap);
+    else if (R >= 2)
+        fold_reduce_kernel<2><<<blocks, 32 * 2, 0, st>>>(pm, pp, D, R, nbins, am, ap);
+    else
+        fold_reduce_kernel<1><<<blocks, 32, 0, st>>>(pm, pp, D, R, nbins, am, ap);
     return cudaGetLastError();
 }
 
