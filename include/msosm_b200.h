@@ -206,8 +206,8 @@ MSOSM_API msosm_status msosm_dedisp_output_device_ptr(msosm_dedisp *d, msosm_com
 
 /* ---- batches: many observations in one launch ---------------------------
  * One filter call of each of n handles (observations of any length, band
- * and trial grid) with one persistent dedispersion launch per group of
- * handles that run the same tensor-core kernel variant (FFT size, operand
+ * and trial grid) with one persistent dedispersion launch per group of up to
+ * 128 handles that run the same tensor-core kernel variant (FFT size, operand
  * type, series/fold): the group's work items (handle, trial, block range)
  * are taken by the CTAs from a counter, largest first, so uneven
  * observations share the GPU without a tail per observation.  Handles of

@@ -9,6 +9,7 @@
 #include <cstring>
 #include <new>
 #include <string>
+#include <memory>
 #include <vector>
 
 #include <cuda_runtime.h>
@@ -1131,18 +1132,15 @@ static msosm_status filter_block(msosm_dedisp *d, const void *input, InputKind k
 
 struct msosm_batch {
     struct Group {
-        std::vector<int> members;  // handle indices, largest work items first
+        std::vector<int> members;  // handle indices, largest work items first (at most kBatchMax)
         std::vector<int> R;        // block ranges per trial of each member in this batch
         int log2n = 0;
         bool bf16 = false, series = false, fold = false;
         size_t fold_smem = 0;
         int grid = 1;
         int items = 0;
-        DedispArgs *args_d = nullptr;   // [n]
-        int *prefix_d = nullptr;        // [n + 1]
         int *counter_d = nullptr;
-        DedispArgs *args_h = nullptr;   // pinned, [2][n]
-        cudaEvent_t ev_args[2] = {nullptr, nullptr};
+        std::unique_ptr<BatchArgs> args;  // the launch's parameter: prefix and arguments
     };
     std::vector<msosm_dedisp *> h;
     std::vector<Group> groups;
@@ -1158,16 +1156,8 @@ static void batch_release(msosm_batch *b)
         return;
     if (b->stream)
         cudaStreamSynchronize(b->stream);
-    for (auto &g : b->groups) {
-        cudaFree(g.args_d);
-        cudaFree(g.prefix_d);
+    for (auto &g : b->groups)
         cudaFree(g.counter_d);
-        if (g.args_h)
-            cudaFreeHost(g.args_h);
-        for (cudaEvent_t e : g.ev_args)
-            if (e)
-                cudaEventDestroy(e);
-    }
     // the handles go back to their own streams
     for (msosm_dedisp *d : b->h)
         if (d->stream == b->stream)
@@ -1219,7 +1209,8 @@ msosm_status msosm_batch_create(msosm_dedisp *const *handles, int n, msosm_batch
         int gi = -1;
         for (size_t k = 0; k < b->groups.size(); ++k) {
             const auto &g = b->groups[k];
-            if (g.log2n == d->log2n && g.bf16 == d->tc_bf16 && g.series == d->series && g.fold == d->fold)
+            if (g.log2n == d->log2n && g.bf16 == d->tc_bf16 && g.series == d->series && g.fold == d->fold &&
+                (int)g.members.size() < kBatchMax)
                 gi = (int)k;
         }
         if (gi < 0) {
@@ -1273,13 +1264,16 @@ msosm_status msosm_batch_create(msosm_dedisp *const *handles, int n, msosm_batch
         g.items = prefix.back();
         g.grid = (int)std::min<long long>(g.items, resident);
         const size_t nm = g.members.size();
-        CKB(cudaMalloc((void **)&g.args_d, sizeof(DedispArgs) * nm));
-        CKB(cudaMalloc((void **)&g.prefix_d, sizeof(int) * (nm + 1)));
         CKB(cudaMalloc((void **)&g.counter_d, sizeof(int)));
-        CKB(cudaMallocHost((void **)&g.args_h, sizeof(DedispArgs) * 2 * nm));
-        CKB(cudaMemcpy(g.prefix_d, prefix.data(), sizeof(int) * (nm + 1), cudaMemcpyHostToDevice));
-        for (cudaEvent_t &e : g.ev_args)
-            CKB(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+        g.args.reset(new (std::nothrow) BatchArgs{});
+        if (!g.args) {
+            batch_release(b);
+            return fail(MSOSM_ERR_OOM, "host allocation");
+        }
+        g.args->nobs = (int)nm;
+        g.args->counter = g.counter_d;
+        for (size_t j = 0; j <= nm; ++j)
+            g.args->prefix[j] = prefix[j];
     }
 #undef CKB
     *out = b;
@@ -1325,31 +1319,21 @@ msosm_status msosm_batch_filter(msosm_batch *b, const void *const *inputs, int i
         if (st != MSOSM_OK)
             return st;
     }
-    const int sb = (int)(b->calls & 1);
     for (auto &g : b->groups) {
         const size_t nm = g.members.size();
-        // the pinned argument staging of two calls ago has been copied
-        CK(cudaEventSynchronize(g.ev_args[sb]));
-        DedispArgs *ah = g.args_h + (size_t)sb * nm;
         std::vector<unsigned long long> l0(nm);
         for (size_t j = 0; j < nm; ++j) {
             msosm_dedisp *d = b->h[g.members[j]];
             l0[j] = d->launches;
             bool done = false;
-            msosm_status st = call_begin(d, inputs[g.members[j]], kind, nullptr, l0[j], ah[j], done);
+            msosm_status st = call_begin(d, inputs[g.members[j]], kind, nullptr, l0[j], g.args->args[j], done);
             if (st != MSOSM_OK)
                 return st;
-            ah[j].R = g.R[j];
+            g.args->args[j].R = g.R[j];
         }
-        CK(cudaMemcpyAsync(g.args_d, ah, sizeof(DedispArgs) * nm, cudaMemcpyHostToDevice, b->stream));
-        CK(cudaEventRecord(g.ev_args[sb], b->stream));
         CK(cudaMemsetAsync(g.counter_d, 0, sizeof(int), b->stream));
-        BatchArgs ba{};
-        ba.args = g.args_d;
-        ba.prefix = g.prefix_d;
-        ba.nobs = (int)nm;
-        ba.counter = g.counter_d;
-        CK(launch_tc_dedisp_batch(g.log2n, g.bf16, g.series, g.fold, ba, g.fold_smem, g.grid, b->stream));
+        // the table travels as the launch's parameter (copied at the launch)
+        CK(launch_tc_dedisp_batch(g.log2n, g.bf16, g.series, g.fold, *g.args, g.fold_smem, g.grid, b->stream));
         for (size_t j = 0; j < nm; ++j) {
             msosm_dedisp *d = b->h[g.members[j]];
             msosm_status st = call_end(d, nullptr, g.R[j], l0[j]);

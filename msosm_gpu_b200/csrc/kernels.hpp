@@ -80,15 +80,23 @@ struct DedispArgs {
     const int *delay_max;     // [D] largest block delay of each trial
 };
 
-// One launch over the work items of many handles (observations) that run the
-// same kernel variant: handle o's items are [prefix[o], prefix[o + 1]), each
-// with args[o]; a CTA takes the next item from *counter (zero before the
-// launch), so items of uneven size balance over the grid.
+// One launch over the work items of up to kBatchMax handles (observations)
+// that run the same kernel variant: handle o's items are [prefix[o],
+// prefix[o + 1]), each with args[o]; a CTA takes the next item from *counter
+// (zero before the launch), so items of uneven size balance over the grid.
+// The table is the kernel's parameter (about 25 KB), so that the kernel reads
+// an item's arguments from the constant bank, as the one-handle kernel reads
+// its own, not from registers.
+constexpr int kBatchMax = 128;
 struct BatchArgs {
-    const DedispArgs *args;  // [nobs], device memory
-    const int *prefix;       // [nobs + 1], device memory
     int nobs;
     int *counter;
+    int prefix[kBatchMax + 1];
+    DedispArgs args[kBatchMax];
+};
+// the one-handle kernel's unused second parameter
+struct NoBatch {
+    int unused;
 };
 
 struct DesignArgs {

@@ -26,6 +26,7 @@
 // the kernel records a nonzero status, waits once more for its last GEMM,
 // frees its tensor memory and returns.
 #include <algorithm>
+#include <type_traits>
 
 #include <cuda_bf16.h>
 #include <cuda_fp16.h>
@@ -339,9 +340,21 @@ __device__ __forceinline__ void pow2_scale_to(float mx, float &s, float &inv)
     inv = __int_as_float((e - X + 1) << 23);
 }
 
+// The arguments of a work item: the launch's own (one handle), or handle o's
+// from the batch's parameter table.
+template <bool MULTI, class B>
+__device__ __forceinline__ const DedispArgs &item_args(const DedispArgs &a0, const B &bt, int o)
+{
+    if constexpr (MULTI)
+        return bt.args[o];
+    else
+        return a0;
+}
+
 template <int LOG2N, class E, bool SERIES, bool FOLD, bool MULTI>
 __global__ void __launch_bounds__(TcShape<LOG2N>::THREADS, TcShape<LOG2N>::CTAS_PER_SM)
-    tc_dedisp_kernel(const __grid_constant__ DedispArgs a0, const __grid_constant__ BatchArgs bt)
+    tc_dedisp_kernel(const __grid_constant__ DedispArgs a0,
+                     const __grid_constant__ std::conditional_t<MULTI, BatchArgs, NoBatch> bt)
 {
     using S = TcShape<LOG2N>;
     constexpr int N = S::N, M = S::M, N2 = S::N2, W = S::WARPS, T = S::THREADS;
@@ -387,49 +400,44 @@ __global__ void __launch_bounds__(TcShape<LOG2N>::THREADS, TcShape<LOG2N>::CTAS_
     // after a timed-out wait.
     // Work items: with one handle, trial w % D, block range w / D of a0, w
     // strided over the grid; in a batch, the next item of any handle from the
-    // counter, its arguments copied into shared memory.  The item body is
-    // written once, inside the loop (as a lambda it cost registers and time).
-    __shared__ DedispArgs sargs;  // batch only
-    __shared__ int swork[2];
+    // counter, its arguments read from the batch's parameter table.  The
+    // item body is written once, inside the loop (as a lambda it cost
+    // registers and time).
+    __shared__ int swork[2];  // batch only
     const int items0 = MULTI ? 0 : a0.D * a0.R;
     for (int it = 0; !failed; ++it) {
-        int w;
+        int w, o = 0;
         if constexpr (!MULTI) {
             w = blockIdx.x + it * gridDim.x;
             if (w >= items0)
                 break;
         } else {
-            __syncthreads();  // every reader of sargs / swork is done
+            __syncthreads();  // every reader of swork is done
             if (tid == 0) {
                 const int gw = atomicAdd(bt.counter, 1);
-                int o = -1;
-                if (gw < __ldg(bt.prefix + bt.nobs)) {
+                int ob_ = -1;
+                if (gw < bt.prefix[bt.nobs]) {
                     int lo = 0, hi = bt.nobs - 1;  // last o with prefix[o] <= gw
                     while (lo < hi) {
                         const int mid = (lo + hi + 1) >> 1;
-                        if (__ldg(bt.prefix + mid) <= gw)
+                        if (bt.prefix[mid] <= gw)
                             lo = mid;
                         else
                             hi = mid - 1;
                     }
-                    o = lo;
+                    ob_ = lo;
                 }
-                swork[0] = o < 0 ? -1 : gw - __ldg(bt.prefix + o);
-                swork[1] = o;
+                swork[0] = ob_ < 0 ? -1 : gw - bt.prefix[ob_];
+                swork[1] = ob_;
             }
             __syncthreads();
-            const int o = swork[1];
+            // warp-uniform by construction (lane 0's copy)
+            o = __shfl_sync(0xffffffffu, swork[1], 0);
             if (o < 0)
                 break;
-            w = swork[0];
-            static_assert(sizeof(DedispArgs) % 4 == 0, "DedispArgs copied as words");
-            const uint32_t *src = reinterpret_cast<const uint32_t *>(bt.args + o);
-            uint32_t *dst = reinterpret_cast<uint32_t *>(&sargs);
-            for (int i = tid; i < (int)(sizeof(DedispArgs) / 4); i += T)
-                dst[i] = src[i];
-            __syncthreads();
+            w = __shfl_sync(0xffffffffu, swork[0], 0);
         }
-        const DedispArgs &a = MULTI ? sargs : a0;
+        const DedispArgs &a = item_args<MULTI>(a0, bt, o);
         if constexpr (MULTI) {
             status = a.status;
             if constexpr (FOLD)
@@ -851,8 +859,8 @@ int tc_blocks_per_sm_t(bool bf16, bool series, bool fold, size_t extra_smem)
     });
 }
 
-template <int LOG2N, bool MULTI>
-cudaError_t launch_tc_t(bool bf16, bool series, bool fold, const DedispArgs &a, const BatchArgs &b,
+template <int LOG2N, bool MULTI, class B>
+cudaError_t launch_tc_t(bool bf16, bool series, bool fold, const DedispArgs &a, const B &b,
                         size_t fold_smem, int grid, cudaStream_t st)
 {
     using S = TcShape<LOG2N>;
@@ -896,7 +904,7 @@ cudaError_t launch_tc_dedisp(int log2n, bool bf16, bool series, bool fold, const
 {
     if (!a.status || !tc_supported(log2n))
         return cudaErrorInvalidValue;
-    const BatchArgs none{};
+    const NoBatch none{};
     const size_t fs = fold ? fold_smem_bytes(a.fold.nbins, a.fold.span_cap, a.fold.smem_prof != 0, tc_threads(log2n))
                            : 0;
     if (log2n == 13)
@@ -907,7 +915,7 @@ cudaError_t launch_tc_dedisp(int log2n, bool bf16, bool series, bool fold, const
 cudaError_t launch_tc_dedisp_batch(int log2n, bool bf16, bool series, bool fold, const BatchArgs &b,
                                    size_t fold_smem, int grid, cudaStream_t st)
 {
-    if (!b.args || !b.prefix || !b.counter || b.nobs < 1 || !tc_supported(log2n))
+    if (!b.counter || b.nobs < 1 || b.nobs > kBatchMax || !tc_supported(log2n))
         return cudaErrorInvalidValue;
     DedispArgs none{};
     if (log2n == 13)
