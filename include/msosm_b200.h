@@ -209,8 +209,8 @@ MSOSM_API msosm_status msosm_dedisp_output_device_ptr(msosm_dedisp *d, msosm_com
  * and trial grid) with one persistent dedispersion launch per group of up to
  * 128 handles that run the same tensor-core kernel variant (FFT size, operand
  * type, series/fold): the group's work items (handle, trial, block range)
- * are taken by the CTAs from a counter, largest first, so uneven
- * observations share the GPU without a tail per observation.  Handles of
+ * are taken by the CTAs from a counter, the largest handle's first, so
+ * uneven observations share the GPU without a tail per observation.  Handles of
  * other kernels (FP32, FFT sizes without a tensor-core transform, the
  * four-step sizes) run their calls one after another in the same batch call.
  * The reference has no counterpart (it dedisperses one observation per
@@ -221,9 +221,8 @@ MSOSM_API msosm_status msosm_dedisp_output_device_ptr(msosm_dedisp *d, msosm_com
  * batch is destroyed); a handle belongs to one batch at a time.  inputs[i]
  * holds count*M samples of handle i (host or device pointers), all of one
  * kind.  Results per handle: msosm_dedisp_get_output_* / get_profiles, as
- * after msosm_dedisp_filter_block_*; a handle's results equal those of its
- * own calls up to the order of the fold's partial sums (the batch may cut a
- * trial into fewer block ranges). */
+ * after msosm_dedisp_filter_block_*: each handle keeps its own work items
+ * (trial, block range), so its results equal those of its own calls. */
 typedef struct msosm_batch msosm_batch;
 #define MSOSM_INPUT_UINT16 0
 #define MSOSM_INPUT_C64 1

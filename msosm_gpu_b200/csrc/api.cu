@@ -1225,13 +1225,13 @@ msosm_status msosm_batch_create(msosm_dedisp *const *handles, int n, msosm_batch
         b->groups[gi].members.push_back(i);
     }
     for (auto &g : b->groups) {
-        // work items of similar size over the whole group: about eight per
-        // resident CTA, each member's block-pair ranges sized to that, never
-        // more ranges than the member's own partial rows hold
-        long long units = 0;
+        // each member keeps its own cut of trials into block ranges and its
+        // item order (range-major, so the CTAs working at one time read the
+        // same ring rows, which stay in L2 for every trial), as in its own
+        // calls; members are ordered largest first, so the last items of the
+        // launch are small ones
         for (int i : g.members) {
             const msosm_dedisp *d = b->h[i];
-            units += (long long)d->D * ((d->count + 1) / 2);
             if (g.fold)
                 g.fold_smem = std::max(g.fold_smem, fold_smem_bytes(d->nbins, d->win_cap, d->nbins <= smem_bins_limit(d),
                                                                     tc_threads(d->log2n)));
@@ -1240,26 +1240,19 @@ msosm_status msosm_batch_create(msosm_dedisp *const *handles, int n, msosm_batch
         if (per_sm < 1)
             per_sm = 1;
         const long long resident = (long long)per_sm * sms;
-        const double per_item = std::max(1.0, (double)units / (8.0 * (double)resident));
-        // largest items first: the counter hands them out in this order
-        std::vector<std::pair<double, int>> order;
+        std::vector<std::pair<long long, int>> order;
         for (int i : g.members) {
             const msosm_dedisp *d = b->h[i];
-            const long long pairs = (d->count + 1) / 2;
-            long long R = (long long)std::llround((double)pairs / per_item);
-            R = std::max(1ll, std::min(R, (long long)d->R));
-            order.push_back({(double)pairs / (double)R, i});
+            order.push_back({(long long)d->D * ((d->count + 1) / 2), i});
         }
         std::stable_sort(order.begin(), order.end(), [](const auto &x, const auto &y) { return x.first > y.first; });
         g.members.clear();
         std::vector<int> prefix(1, 0);
         for (const auto &o : order) {
             const msosm_dedisp *d = b->h[o.second];
-            const long long pairs = (d->count + 1) / 2;
-            const int R = (int)std::max(1ll, std::min((long long)d->R, (long long)std::llround((double)pairs / o.first)));
             g.members.push_back(o.second);
-            g.R.push_back(R);
-            prefix.push_back(prefix.back() + d->D * R);
+            g.R.push_back(d->R);
+            prefix.push_back(prefix.back() + d->D * d->R);
         }
         g.items = prefix.back();
         g.grid = (int)std::min<long long>(g.items, resident);

@@ -2,7 +2,8 @@
 of different length, band, trial grid and FFT size dedispersed by one
 persistent tensor-core launch per kernel group, every observation's series
 and folded profiles against the FP64 oracle (the tensor path's bounds) and
-against the same observation run through its own handle.  An FP32 handle in
+against the same observation run through its own handle (the batch keeps
+each handle's own work items, so the two agree to rounding).  An FP32 handle in
 the same batch runs its own launch inside the batch call."""
 import numpy as np
 import pytest
@@ -61,7 +62,8 @@ def test_batch_matches_oracle_and_own_handles():
                 tol = SERIES_TOL if OBS[i][5] != "fp32" else 2e-5
                 e = rel_rms(y[t], ref[t])
                 assert e < tol, (i, t, c, e)
-                assert rel_rms(y[t], ys[t]) < tol, (i, t, c)
+                # the same work items as the handle's own calls: equal to rounding
+                assert rel_rms(y[t], ys[t]) < 1e-6, (i, t, c, rel_rms(y[t], ys[t]))
                 worst[i] = max(worst.get(i, 0.0), e)
     for i, (d, s) in enumerate(zip(batch_h, solo_h)):
         p, ps = d.get_profiles().astype(np.float64), s.get_profiles().astype(np.float64)
@@ -69,7 +71,7 @@ def test_batch_matches_oracle_and_own_handles():
         assert d.folded_periods() == s.folded_periods() > 0
         for t in range(d.numDMs):
             assert rel_rms(p[t], pr[t]) < (FOLD_TOL if OBS[i][5] != "fp32" else 2e-5), (i, t)
-            assert rel_rms(p[t], ps[t]) < FOLD_TOL, (i, t)
+            assert rel_rms(p[t], ps[t]) < 1e-6, (i, t)
     b.synchronize()
     b.close()
     # the handles go back to their own streams and keep working
