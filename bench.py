@@ -187,7 +187,7 @@ def cpu_baseline(dms, x, budget_s=12.0):
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import cpu_fp32 as C
     threads = os.cpu_count() or 1
-    count = 16
+    count = 64  # calls of 131k samples: smaller calls leave it bound by per-task overhead
     c = C.MsosmFP32(BW, dms, F0, FFTPOINT, count, period=PULSAR["period"], time_bin=NBINS, threads=threads)
     blk = count * c.M
 
