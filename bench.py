@@ -517,7 +517,7 @@ def run_ours(args):
 
 
 # ---------------------------------------------------------------------------
-# precision sweep: 64 MHz band centred at 1400 MHz, FFT 8192, 1024 trials
+# precision sweep: 64 MHz band centred at 1400 MHz, FFT 8192 (--fftpoint), 1024 trials
 # ---------------------------------------------------------------------------
 
 SWEEP = dict(bw=64e6, f0=1368e6, fftpoint=8192, n_dm=1024, dm_max=200.0, log2_samples=26, nbins=1024,
@@ -708,7 +708,7 @@ UNEVEN = dict(n_obs=64, log2_len=(20, 25), bws=(4e6, 16e6, 32e6, 64e6), centre=(
               trials=(16, 512), dm_max=(20.0, 300.0), period=(1e-3, 1.0), duty=(0.01, 0.10),
               snr=(0.02, 0.2), nbins=256, seed=0)
 FIXED = [(2048, "fp32"), (4096, "fp32"), (8192, "fp32"), (16384, "fp32"), (32768, "fp32"), (4096, "fp16"),
-         (8192, "fp16")]
+         (8192, "fp16"), (16384, "fp16")]
 
 
 def uneven_observations(n_obs, seed):
@@ -739,17 +739,23 @@ def uneven_observations(n_obs, seed):
     return obs
 
 
-def uneven_one_launch(obs, tuned, cfg, stream, total_units, reps=3):
+def uneven_one_launch(obs, tuned, cfg, stream, reps=3):
     """The tuned configuration of every observation as one batch
     (DedispBatch: one persistent launch per tensor-core kernel group, work
     items handed out largest first), against the same handles called back to
     back on the same stream; device-resident inputs, CUDA events, the
-    median of `reps` calls each after one warm-up call."""
+    median of `reps` calls each after one warm-up call.  Observations tuned
+    to an FFT above one thread block (the FP32 four-step path, above 16384
+    points) are left out: a batch runs them in their own launches anyway,
+    and their per-trial transform buffers (trials x blocks x FFT points)
+    held for all observations at once would not fit the device."""
     import torch
     from msosm_gpu_b200 import DedispBatch, Dedisperser
     from msosm_gpu_b200 import simulator as G
+    keep = [k for k, (n, _) in enumerate(tuned) if n <= 16384]
+    units = float(sum(obs[k]["trials"] * obs[k]["n"] for k in keep))
     handles, inputs = [], []
-    for o, (n, p) in zip(obs, tuned):
+    for o, (n, p) in ((obs[k], tuned[k]) for k in keep):
         dms = np.linspace(0.0, o["dm_max"], o["trials"]).astype(np.float32)
         inputs.append(G.pulsar_baseband(o["n"], o["bw"], o["f0"], o["dm"], o["period"], o["duty"], o["snr"],
                                         seed=o["i"], device=torch.device("cuda")))
@@ -788,9 +794,11 @@ def uneven_one_launch(obs, tuned, cfg, stream, total_units, reps=3):
         d.close()
     del inputs
     torch.cuda.empty_cache()
-    return {"ms": batch_ms, "value": total_units / (batch_ms * 1e-3) / 1e6,
-            "back_to_back_ms": seq_ms, "back_to_back_value": total_units / (seq_ms * 1e-3) / 1e6,
+    return {"ms": batch_ms, "value": units / (batch_ms * 1e-3) / 1e6,
+            "back_to_back_ms": seq_ms, "back_to_back_value": units / (seq_ms * 1e-3) / 1e6,
             "speedup_vs_back_to_back": seq_ms / batch_ms, "batch": info,
+            "observations": len(keep), "left_out_above_16384": len(obs) - len(keep),
+            "dm_trial_samples": units,
             "method": "the tuned handles of all observations; one DedispBatch call (one persistent launch per "
                       "tensor-core kernel group, forward transforms per observation) against one filter_block "
                       "call per observation on the same stream; device-resident inputs, CUDA events, median of "
@@ -858,7 +866,7 @@ def run_uneven_batch(args):
         log(f"obs {o['i']}: n={o['n']} bw={o['bw'] / 1e6:g} D={o['trials']} dm_max={o['dm_max']:.0f} "
             f"tuned={ch.fftpoint}/{ch.precision} " + " ".join(f"{k[0]}/{k[1]}={v:.1f}" for k, v in sorted(res.items())))
     tuned_ms = sum(r[c] for r, c in zip(times, tuned))
-    one_launch = uneven_one_launch(obs, tuned, cfg, stream, total_units)
+    one_launch = uneven_one_launch(obs, tuned, cfg, stream)
     fixed = {}
     for n, p in FIXED:
         ms = 0.0
@@ -1405,7 +1413,13 @@ def main():
     ap.add_argument("--min-coherence", type=float, default=None,
                     help="uneven-batch: the autotuner's floor on MS-OSM coherence with exact dedispersion")
     ap.add_argument("--seeds", type=int, default=SWEEP["seeds"], help="precision-sweep: signal seeds")
+    ap.add_argument("--fftpoint", type=int, default=None, choices=[4096, 8192, 16384],
+                    help="precision-sweep: FFT size (default 8192; each of these runs on the tensor cores)")
     args = ap.parse_args()
+    if args.fftpoint:
+        if args.workload != "precision-sweep":
+            ap.error("--fftpoint applies to the precision-sweep workload")
+        SWEEP["fftpoint"] = args.fftpoint
     if args.workload == "precision-sweep" and args.impl == "reference-gpu":
         args.log2_samples = args.log2_samples or SWEEP["log2_samples"]
         args.dms = args.dms or SWEEP["n_dm"]

@@ -128,8 +128,8 @@ typedef struct msosm_dedisp msosm_dedisp;
 #define MSOSM_FLAG_NO_SERIES 0x2u /* do not materialise the dedispersed series (fold only) */
 /* Inverse transforms on the tensor cores: f16 operands with a power-of-two
  * scale per work item, f32 accumulation.  No counterpart in the reference
- * (its inverse transform is the FP32 cuFFT).  FFT sizes 4096 and 8192 (other
- * sizes return MSOSM_ERR_UNSUPPORTED).  Relative RMS error of the series
+ * (its inverse transform is the FP32 cuFFT).  FFT sizes 4096, 8192 and
+ * 16384 (other sizes return MSOSM_ERR_UNSUPPORTED).  Relative RMS error of the series
  * against FP64: about 5e-4; folded profiles much lower. */
 #define MSOSM_FLAG_TENSOR_F16 0x4u
 /* As MSOSM_FLAG_TENSOR_F16 with bf16 operands (no scaling needed; relative
@@ -558,7 +558,9 @@ MSOSM_API msosm_status msosm_dedisp_set_tc_wait_limit(msosm_dedisp *d, long long
  * with rows [Re | Im] of the input index and columns [Re | Im] of the output
  * frequency.  Step 1: the 64-point DFT of FFT 4096 (K 128, 128 columns);
  * step 2: the 64-point DFT restricted to frequencies 32..63 (K 128, 64
- * columns); step 3: the 128-point DFT of FFT 8192 (K 256, 256 columns).
+ * columns); step 3: the 128-point DFT of FFT 8192 and 16384 (K 256, 256
+ * columns); step 4: the 128-point DFT restricted to frequencies 64..127, the
+ * second GEMM of FFT 16384 (K 256, 128 columns).
  * d: host, 128 x columns floats, row-major.  Needs a GPU. */
 MSOSM_API msosm_status msosm_tc_gemm_check(int step, const uint16_t *a, float *d);
 

@@ -47,7 +47,7 @@ using uint16_pair = msosm_uint16_pair;
 
 // Not in the reference: MS-OSM objects initialised after use_tensor_cores(true)
 // run their inverse transforms on the tensor cores (MSOSM_FLAG_TENSOR_F16: f16
-// operands, f32 accumulation, FFT sizes 4096 and 8192; series error ~5e-4
+// operands, f32 accumulation, FFT sizes 4096, 8192 and 16384; series error ~5e-4
 // relative RMS, folded profiles ~3e-5).  Off by default.
 inline unsigned int &extra_flags()
 {

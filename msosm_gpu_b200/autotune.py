@@ -7,8 +7,8 @@ against FP64 fits the budget:
 * FFT sizes 2^11 .. 2^15 at or above the MS-OSM minimum 2 M_min (smaller
   sizes are raised to it, msosm_gpu_dm_concurrent.cpp:33-35, so they are the
   same candidate);
-* the FP32 CUDA-core kernel at every size; the tensor-core kernel at 4096 and
-  8192 with f16 operands (folded-profile error ~2e-5, series ~5e-4) and with
+* the FP32 CUDA-core kernel at every size; the tensor-core kernel at 4096,
+  8192 and 16384 with f16 operands (folded-profile error ~2e-5, series ~5e-4) and with
   bf16 operands (profiles ~1.3e-3, series ~4e-3) when the budget admits it.
 
 Each candidate runs `calls` timed filter_block calls (after one warm-up) of
@@ -41,7 +41,7 @@ from .prepare import msosm_min_order as min_order_msosm, nd
 # relative RMS error of the folded profiles against FP64, per path (measured
 # on the 64 MHz / FFT 8192 precision sweep and the tensor-core parity tests)
 PROFILE_ERROR = {"fp32": 1e-6, "fp16": 3e-5, "bf16": 2e-3}
-TENSOR_SIZES = (4096, 8192)
+TENSOR_SIZES = (4096, 8192, 16384)
 # 1 - rho = COHERENCE_SLOPE sqrt(Nd) / M, fitted to the FP64 oracle
 # (tests/test_msosm_coherence_cpu.py pins it within 25 %)
 COHERENCE_SLOPE = 0.24

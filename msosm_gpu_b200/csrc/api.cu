@@ -236,9 +236,9 @@ msosm_status design_filters(int log2n, const std::vector<ChirpParams> &cp, float
 }
 
 // Profiles of up to this many bins live in shared memory inside the fused
-// kernel (beyond it, in the global partial rows): the 8192-point tensor-core
-// kernel leaves room for 2048.
-int smem_bins_limit(const msosm_dedisp *d) { return d->tc && d->log2n == 13 ? 2048 : kMaxSmemBins; }
+// kernel (beyond it, in the global partial rows): the 8192- and 16384-point
+// tensor-core kernels leave room for 2048.
+int smem_bins_limit(const msosm_dedisp *d) { return d->tc && d->log2n >= 13 ? 2048 : kMaxSmemBins; }
 
 // Persistent grid of the dedispersion kernel: work items (block range,
 // trial), about eight per resident CTA, spread evenly over the waves.
@@ -258,8 +258,9 @@ cudaError_t plan_grid(msosm_dedisp *d)
         per_sm = 1;
     const long long resident = (long long)per_sm * sms;
     long long R = (8 * resident + d->D - 1) / d->D;
-    // the tensor-core kernel works on pairs of blocks
-    const long long units = d->tc ? (d->count + 1) / 2 : d->count;
+    // the tensor-core kernel works in steps of a pair of blocks (one block at 16384)
+    const int bps = d->tc ? tc_blocks_per_step(d->log2n) : 1;
+    const long long units = (d->count + bps - 1) / bps;
     if (R > units)
         R = units;
     if (R < 1)
@@ -602,7 +603,7 @@ msosm_status msosm_dedisp_create(const float *bw, const float *dm, const float *
     }
     if (d->tc && !tc_supported(log2n)) {
         release(d);
-        return fail(MSOSM_ERR_UNSUPPORTED, "the tensor-core path needs FFT size 4096 or 8192 (got %lu)", 2 * M);
+        return fail(MSOSM_ERR_UNSUPPORTED, "the tensor-core path needs FFT size 4096, 8192 or 16384 (got %lu)", 2 * M);
     }
     if (input_size != 0)
         count = (int)(input_size / M);
@@ -1243,7 +1244,8 @@ msosm_status msosm_batch_create(msosm_dedisp *const *handles, int n, msosm_batch
         std::vector<std::pair<long long, int>> order;
         for (int i : g.members) {
             const msosm_dedisp *d = b->h[i];
-            order.push_back({(long long)d->D * ((d->count + 1) / 2), i});
+            const int bps = tc_blocks_per_step(d->log2n);
+            order.push_back({(long long)d->D * ((d->count + bps - 1) / bps), i});
         }
         std::stable_sort(order.begin(), order.end(), [](const auto &x, const auto &y) { return x.first > y.first; });
         g.members.clear();
@@ -1925,12 +1927,12 @@ msosm_status msosm_fold_planner_chunk(msosm_fold_planner *p, unsigned long size,
 
 msosm_status msosm_tc_gemm_check(int step, const uint16_t *a, float *d)
 {
-    if (step < 1 || step > 3 || !a || !d)
-        return fail(MSOSM_ERR_BAD_ARG, "step must be 1, 2 or 3; a and d non-null");
+    if (step < 1 || step > 4 || !a || !d)
+        return fail(MSOSM_ERR_BAD_ARG, "step must be 1 .. 4; a and d non-null");
     if (msosm_device_count() == 0)
         return fail(MSOSM_ERR_NO_DEVICE, "no CUDA device");
-    const size_t na = (size_t)128 * (step == 3 ? 256 : 128);
-    const size_t nd = (size_t)128 * (step == 3 ? 256 : (step == 1 ? 128 : 64));
+    const size_t na = (size_t)128 * (step >= 3 ? 256 : 128);
+    const size_t nd = (size_t)128 * (step == 3 ? 256 : (step == 2 ? 64 : 128));
     uint16_t *ad = nullptr;
     float *dd = nullptr;
     int *st = nullptr;

@@ -80,7 +80,7 @@ __global__ void __launch_bounds__(FftShape<LOG2N>::T) forward_kernel(FwdArgs a)
     run_stages<LOG2N, -1, PP>(v, buf0, buf1, tid, a.tw);
     const int slot_row = (int)((a.k0 + c) & (a.S - 1));
     float2 *row = a.ring + (size_t)slot_row * N;
-    if ((LOG2N == 12 || LOG2N == 13) && a.tc_order) {
+    if ((LOG2N >= 12 && LOG2N <= 14) && a.tc_order) {
         float mx = 0.f;
 #pragma unroll
         for (int slot = 0; slot < 16; ++slot) {

@@ -23,7 +23,7 @@ struct FwdArgs {
     long long k0;           // global index of this call's first block
     int count;
     const float2 *tw;       // exp(-2 pi i e/N)
-    int tc_order;           // 1: rows in tensor-core order (4096-point only)
+    int tc_order;           // 1: rows in tensor-core order (4096..16384 points)
     float *row_max;         // tc_order: [S] largest |component| of each ring row
 };
 
@@ -141,13 +141,16 @@ int fold_series_block();
 cudaError_t launch_fold_series(const float *I, long long n, int R, const FoldArgs &f, int grid, int trials,
                                cudaStream_t st);
 
-// ---- tensor-core (tcgen05) dedispersion, 4096- and 8192-point transforms (tc_dedisp.cu)
+// ---- tensor-core (tcgen05) dedispersion, 4096-, 8192- and 16384-point transforms (tc_dedisp.cu)
 bool tc_supported(int log2n);
 // threads per CTA of the tensor-core kernel (its fold group size)
 int tc_threads(int log2n);
+// blocks one step of the kernel transforms: 2 (a pair) at 4096 and 8192, 1 at 16384
+int tc_blocks_per_step(int log2n);
 int tc_blocks_per_sm(int log2n, bool bf16, bool series, bool fold, size_t extra_smem);
 // a.H and a.delays in tensor-core order (tc_layout.hpp), ring written with
-// FwdArgs::tc_order; a.R counts ranges of block pairs; bf16: bf16 operands
+// FwdArgs::tc_order; a.R counts ranges of steps (tc_blocks_per_step blocks
+// each); bf16: bf16 operands
 // (else f16)
 cudaError_t launch_tc_dedisp(int log2n, bool bf16, bool series, bool fold, const DedispArgs &a, int grid,
                              cudaStream_t st);

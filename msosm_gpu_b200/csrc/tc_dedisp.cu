@@ -1,5 +1,5 @@
 // tc_dedisp.cu -- tensor-core (tcgen05) variant of the fused dedispersion
-// kernel for 4096-point transforms.
+// kernel for 4096-, 8192- and 16384-point transforms.
 //
 // Same semantics as dedisp_kernel (kernels.cu), which replaces
 // ComplexMultiplyDelay_concurrent_batch + inverse cufftExecC2C +
@@ -7,10 +7,11 @@
 // host fold of Fold_GPU (folding/fold_gpu.cpp:48-194): per (trial, block)
 // gather X[k - delay[b]][b] * H[b] from the spectrum ring, inverse transform,
 // keep outputs m >= M, write the series and/or detect and fold.  Here the
-// inverse transform of two consecutive blocks of one trial runs as two f16
-// GEMMs with f32 accumulation in tensor memory (factorisation and layouts in
-// tc_layout.hpp): GEMM 1 (M 128 = 2 blocks x 64 k1, N 128, K 128), a twiddle
-// pass on the CUDA cores, GEMM 2 (M 128 = 2 blocks x 64 m2, N 64, K 128).
+// inverse transform of a step (two consecutive blocks of one trial at 4096
+// and 8192 points, one block at 16384) runs as two f16 GEMMs with f32
+// accumulation in tensor memory (factorisation and layouts in tc_layout.hpp):
+// at 4096 GEMM 1 (M 128 = 2 blocks x 64 k1, N 128, K 128), a twiddle pass on
+// the CUDA cores, GEMM 2 (M 128 = 2 blocks x 64 m2, N 64, K 128).
 //
 // Precision: the gathered products of a work item (one trial, a range of
 // blocks) are scaled by a power of two chosen so that no component can reach
@@ -217,6 +218,8 @@ __device__ __forceinline__ float warp_max(float v)
 //     n >= N2 -> sin(2 pi k2 (n - N2) / N2)           (output frequency m2)
 //   GEMM 2, B2[n][k1], k1 < 64: n < 32 -> cos(2 pi k1 (32 + n) / 64),
 //     n >= 32 -> sin(2 pi k1 n / 64)                   (output m1 = 32..63)
+// At N = 16384 (N1 = N2 = 128) GEMM 2 reads B1's columns 64..127 (C) and
+// 192..255 (S) instead of a B2.
 template <class E, int LOG2N>
 __device__ void fill_constants(unsigned char *sm, int tid)
 {
@@ -228,7 +231,7 @@ __device__ void fill_constants(unsigned char *sm, int tid)
         sincospif((float)((k * (n & (N2 - 1))) & (N2 - 1)) * (2.0f / N2), &s, &c);
         *reinterpret_cast<typename E::h1 *>(sm + S::SMEM_B1 + k_off(n, k, (int)S::SBO_B1)) = E::one(n < N2 ? c : s);
     }
-    for (int e = tid; e < 64 * 64; e += (int)blockDim.x) {
+    for (int e = tid; e < (S::B2_BYTES ? 64 * 64 : 0); e += (int)blockDim.x) {
         const int n = e >> 6, k = e & 63;
         float s, c;
         sincospif((float)((k * (32 + (n & 31))) & 63) * (1.0f / 32.0f), &s, &c);
@@ -292,7 +295,29 @@ __device__ __forceinline__ void issue_cgemm(uint32_t tmem_d, uint32_t a, uint32_
                 smem_desc(b + s * kDescStepB, 128, sbo), id_half, 1u);
 }
 
-// GEMM 1 of a pair (operand buffer at a), committed to bar
+// The same complex GEMM with C and S at separate places (bc, bs; N = half
+// columns each): Re x C, Re x S, then -Im x S, Im x C.
+template <class E>
+__device__ __forceinline__ void issue_cgemm_cs(uint32_t tmem_d, uint32_t a, uint32_t bc, uint32_t bs, int half,
+                                               int ksteps, uint32_t sbo)
+{
+    const uint32_t id_neg = idesc_f16(128, half, true, true, E::fmt);
+    const uint32_t id_half = idesc_f16(128, half, true, false, E::fmt);
+    for (int s = 0; s < ksteps; ++s)
+        mma_f16(tmem_d, smem_desc(a + s * kDescStepA, 2048, 128), smem_desc(bc + s * kDescStepB, 128, sbo), id_half,
+                s > 0 ? 1u : 0u);
+    for (int s = 0; s < ksteps; ++s)
+        mma_f16(tmem_d + half, smem_desc(a + s * kDescStepA, 2048, 128), smem_desc(bs + s * kDescStepB, 128, sbo),
+                id_half, s > 0 ? 1u : 0u);
+    for (int s = 0; s < ksteps; ++s)
+        mma_f16(tmem_d, smem_desc(a + (ksteps + s) * kDescStepA, 2048, 128),
+                smem_desc(bs + s * kDescStepB, 128, sbo), id_neg, 1u);
+    for (int s = 0; s < ksteps; ++s)
+        mma_f16(tmem_d + half, smem_desc(a + (ksteps + s) * kDescStepA, 2048, 128),
+                smem_desc(bc + s * kDescStepB, 128, sbo), id_half, 1u);
+}
+
+// GEMM 1 of a step (operand buffer at a), committed to bar
 template <class E, int LOG2N>
 __device__ __forceinline__ void issue_gemm1(uint32_t tmem, uint32_t s0, uint32_t a, uint32_t bar)
 {
@@ -301,16 +326,22 @@ __device__ __forceinline__ void issue_gemm1(uint32_t tmem, uint32_t s0, uint32_t
     mma_commit(bar);
 }
 
-// GEMM 2 of a pair: one GEMM for both blocks at N = 4096 (rows 64 b + m2),
+// GEMM 2 of a step: one GEMM for both blocks at N = 4096 (rows 64 b + m2),
 // one per block at N = 8192 (block b's operand 32 KB on, its result 64
-// columns on), committed to bar
+// columns on), one for the block at N = 16384 (K = 128 k1, its C and S
+// columns of B1), committed to bar
 template <class E, int LOG2N>
 __device__ __forceinline__ void issue_gemm2(uint32_t tmem, uint32_t s0, uint32_t a, uint32_t bar)
 {
     using S = TcShape<LOG2N>;
-    issue_cgemm<E>(tmem + S::D2_COL, a, s0 + S::SMEM_B2, 32, 4, 1024);
-    if constexpr (S::N2 == 128)
-        issue_cgemm<E>(tmem + S::D2_COL + 64, a + 32768, s0 + S::SMEM_B2, 32, 4, 1024);
+    if constexpr (S::N1 == 128) {
+        issue_cgemm_cs<E>(tmem + S::D2_COL, a, s0 + S::SMEM_B1 + 8 * S::SBO_B1, s0 + S::SMEM_B1 + 24 * S::SBO_B1,
+                          S::D2_HALF, S::N1 / 16, S::SBO_B1);
+    } else {
+        issue_cgemm<E>(tmem + S::D2_COL, a, s0 + S::SMEM_B2, 32, 4, 1024);
+        if constexpr (S::N2 == 128)
+            issue_cgemm<E>(tmem + S::D2_COL + 64, a + 32768, s0 + S::SMEM_B2, 32, 4, 1024);
+    }
     mma_commit(bar);
 }
 
@@ -357,7 +388,7 @@ __global__ void __launch_bounds__(TcShape<LOG2N>::THREADS, TcShape<LOG2N>::CTAS_
                      const __grid_constant__ std::conditional_t<MULTI, BatchArgs, NoBatch> bt)
 {
     using S = TcShape<LOG2N>;
-    constexpr int N = S::N, M = S::M, N2 = S::N2, W = S::WARPS, T = S::THREADS;
+    constexpr int N = S::N, M = S::M, N1 = S::N1, N2 = S::N2, W = S::WARPS, T = S::THREADS, BPS = S::BPS;
     extern __shared__ __align__(1024) unsigned char sm[];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t s0 = smem_addr(sm);
@@ -373,11 +404,12 @@ __global__ void __launch_bounds__(TcShape<LOG2N>::THREADS, TcShape<LOG2N>::CTAS_
     const uint32_t tD1 = tmem + lane_base, tD2 = tmem + lane_base + S::D2_COL;
     const int g = warp >> 2;
     const int row = 32 * (warp & 3) + lane;
-    const int rb = row >> 6, ri = row & 63;  // GEMM 1 row: block of the pair, k1
-    // GEMM 2 rows: N = 4096 -> (block rb, m2 = ri); N = 8192 -> (block g % 2, m2 = row)
-    const int ob = N2 == 64 ? rb : (g & 1);
+    const int rb = N1 == 128 ? 0 : row >> 6, ri = row & (N1 - 1);  // GEMM 1 row: block of the step, k1
+    // GEMM 2 rows: N = 4096 -> (block rb, m2 = ri); N = 8192 -> (block g % 2,
+    // m2 = row); N = 16384 -> (the step's one block, m2 = row)
+    const int ob = N2 == 64 ? rb : (BPS == 2 ? (g & 1) : 0);
     const int om2 = N2 == 64 ? ri : row;
-    const int oh = N2 == 64 ? g : (g >> 1);  // output columns c = 16 oh .. 16 oh + 15
+    const int oh = N2 == 64 || BPS == 1 ? g : (g >> 1);  // output columns c = 16 oh .. 16 oh + 15
     const uint32_t tD2b = tD2 + (N2 == 64 ? 0u : 64u * (uint32_t)ob);
     // this thread's twiddles e^{+2 pi i ri m2 / N}, m2 = 32 g + i, as 16-bit
     // pairs (m2, m2 + 1) matching the operand packing
@@ -445,24 +477,30 @@ __global__ void __launch_bounds__(TcShape<LOG2N>::THREADS, TcShape<LOG2N>::CTAS_
         }
         const float4 *__restrict__ ring4 = reinterpret_cast<const float4 *>(a.ring);
         const float2 *__restrict__ ring2 = a.ring;
-        const int npairs = (a.count + 1) >> 1;
+        const int nunits = (a.count + BPS - 1) >> (BPS - 1);  // steps of the whole call
         const unsigned long long wlim = (unsigned long long)a.wait_limit_ns;
         const int smask = a.S - 1;
         const int dm = w % a.D;
         const int rr = w / a.D;
-        const int kb = 2 * (int)((long long)npairs * rr / a.R);
-        const int ke = min(a.count, 2 * (int)((long long)npairs * (rr + 1) / a.R));
-        const int np = (ke - kb + 1) >> 1;
-        // this thread's bin pairs: filter values and delays, fixed for the trial
-        float4 hreg[8];
-        uint32_t dd[8];
+        const int kb = BPS * (int)((long long)nunits * rr / a.R);
+        const int ke = min(a.count, BPS * (int)((long long)nunits * (rr + 1) / a.R));
+        const int np = (ke - kb + BPS - 1) >> (BPS - 1);
+        // this thread's bin pairs: delays, fixed for the trial (one row half at
+        // 4096 and 8192, both at 16384), and at 4096 and 8192 the filter values
+        // too (at 16384 they would take 64 registers: read with each step)
+        constexpr int NH = 2 / BPS;
+        const float4 *__restrict__ H4 = reinterpret_cast<const float4 *>(a.H + (size_t)dm * N);
+        float4 hreg[BPS == 2 ? 8 : 1];
+        uint32_t dd[8 * NH];
         {
-            const float4 *__restrict__ H4 = reinterpret_cast<const float4 *>(a.H + (size_t)dm * N);
             const uint32_t *__restrict__ dl2 = reinterpret_cast<const uint32_t *>(a.delays + (size_t)dm * N);
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
-                dd[j] = __ldg(dl2 + (j * W + warp) * 32 + lane);
-                hreg[j] = __ldg(H4 + (j * W + warp) * 32 + lane);
+#pragma unroll
+                for (int h = 0; h < NH; ++h)
+                    dd[NH * j + h] = __ldg(dl2 + h * (N / 4) + (j * W + warp) * 32 + lane);
+                if constexpr (BPS == 2)
+                    hreg[j] = __ldg(H4 + (j * W + warp) * 32 + lane);
             }
         }
         // power-of-two scale of the work item: |Z| <= 2 max|X| max|H| over
@@ -483,9 +521,11 @@ __global__ void __launch_bounds__(TcShape<LOG2N>::THREADS, TcShape<LOG2N>::CTAS_
             for (int i = 0; i < W; ++i)
                 wm = fmaxf(wm, wmax[i]);
             pow2_scale_to<S::SCALE_EXP>(2.0f * wm * __ldg(a.h_max + dm), sc, isc);
+            if constexpr (BPS == 2) {
 #pragma unroll
-            for (int j = 0; j < 8; ++j)
-                hreg[j] = make_float4(hreg[j].x * sc, hreg[j].y * sc, hreg[j].z * sc, hreg[j].w * sc);
+                for (int j = 0; j < 8; ++j)
+                    hreg[j] = make_float4(hreg[j].x * sc, hreg[j].y * sc, hreg[j].z * sc, hreg[j].w * sc);
+            }
         }
         int sp = 0, sbase = 0, scnt = 0;
         if constexpr (FOLD) {
@@ -500,15 +540,78 @@ __global__ void __launch_bounds__(TcShape<LOG2N>::THREADS, TcShape<LOG2N>::CTAS_
             span_refill(a.fold, fw, sp, sbase, scnt);
         }
 
-        // Gather pair i of the item (blocks k, k + 1) into operand buffer
-        // `op`: Z = X[kg + b - delay][bin] * H[bin] * sc, element (row 64 b
-        // + k1, k = k2) of the MN-major operand, Im parts N2 K-columns on.
+        // Gather step i of the item into operand buffer `op`: Z = X[kg + b -
+        // delay][bin] * H[bin] * sc, element (row 64 b + k1, k = k2) of the
+        // MN-major operand for blocks k, k + 1 (4096, 8192), element (row
+        // 64 h + k1 mod 64, k = k2) for row half h of block k (16384); Im
+        // parts N2 K-columns on.
         auto gather = [&](int i, unsigned char *op) {
-            const int k = kb + 2 * i;
-            const bool two = k + 1 < ke;
+            const int k = kb + BPS * i;
+            const bool two = BPS == 2 && k + 1 < ke;
             const long long kg = a.k0 + k;
             const int slot0 = (int)(kg & smask);
-            if (kg >= a.max_delay && two) {
+            // the scaled product of a bin pair, stored as row-pair words of
+            // core-matrix row group 8 b + j
+            auto put = [&](int j, int b, const float4 &x, const float4 &hv, float f) {
+                const float zr0 = (x.x * hv.x - x.y * hv.y) * f, zi0 = (x.x * hv.y + x.y * hv.x) * f;
+                const float zr1 = (x.z * hv.z - x.w * hv.w) * f, zi1 = (x.z * hv.w + x.w * hv.z) * f;
+                const int off = (b * 8 + j) * 128 + warp * 2048 + (lane >> 2) * 16 + (lane & 3) * 4;
+                *reinterpret_cast<uint32_t *>(op + off) = pack2<E>(zr0, zr1);
+                *reinterpret_cast<uint32_t *>(op + off + S::IM_OFF) = pack2<E>(zi0, zi1);
+            };
+            if constexpr (BPS == 1) {
+                if (kg >= a.max_delay) {
+                    // as the pair gather below, over the two row halves of
+                    // one block in turn, with the filter read alongside the
+                    // ring (both halves' loads in flight at once spilled
+                    // twice as much and took 21 % longer)
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        float4 xa[8], hv[8];
+                        float2 xb[8];
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) {
+                            const int q = h * (N / 4) + (j * W + warp) * 32 + lane;
+                            const uint32_t d = dd[2 * j + h];
+                            const int r0 = (slot0 - (int)(d & 0xFFFFu)) & smask;
+                            const int r1 = (slot0 - (int)(d >> 16)) & smask;
+                            xa[j] = ring4[(size_t)r0 * (N / 2) + q];
+                            xb[j] = r1 != r0 ? ring2[(size_t)r1 * N + 2 * q + 1] : make_float2(0.f, 0.f);
+                            hv[j] = __ldg(H4 + q);
+                        }
+#pragma unroll
+                        for (int j = 0; j < 8; ++j) {
+                            const uint32_t d = dd[2 * j + h];
+                            const bool split = (d & 0xFFFFu) != (d >> 16);
+                            const float4 x = split ? make_float4(xa[j].x, xa[j].y, xb[j].x, xb[j].y) : xa[j];
+                            put(j, h, x, hv[j], sc);
+                        }
+                    }
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 8; ++j) {
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) {
+                            const int q = h * (N / 4) + (j * W + warp) * 32 + lane;
+                            const uint32_t d = dd[2 * j + h];
+                            const int d0 = (int)(d & 0xFFFFu), d1 = (int)(d >> 16);
+                            float4 x = make_float4(0.f, 0.f, 0.f, 0.f);
+                            // blocks before the stream start are zero
+                            if (kg >= d0) {
+                                const float2 t = ring2[(size_t)((slot0 - d0) & smask) * N + 2 * q];
+                                x.x = t.x;
+                                x.y = t.y;
+                            }
+                            if (kg >= d1) {
+                                const float2 t = ring2[(size_t)((slot0 - d1) & smask) * N + 2 * q + 1];
+                                x.z = t.x;
+                                x.w = t.y;
+                            }
+                            put(j, h, x, __ldg(H4 + q), sc);
+                        }
+                    }
+                }
+            } else if (kg >= a.max_delay && two) {
                 // every delayed block exists: no zero fill.  No branch on the
                 // delays, so all loads of the pair issue before the first use:
                 // each bin pair as one float4 from the first bin's row, and,
@@ -578,7 +681,7 @@ __global__ void __launch_bounds__(TcShape<LOG2N>::THREADS, TcShape<LOG2N>::CTAS_
 
         // D1 -> twiddle (16-bit arithmetic) -> 16-bit operand of GEMM 2 in
         // `op`: rows (N = 4096: 64 rb +) m2, m2 = 32 g + 16 p + 8 q + 0..7;
-        // k = k1 (Re), 64 + k1 (Im); at N = 8192 block rb's operand 32 KB on
+        // k = k1 (Re), N1 + k1 (Im); at N = 8192 block rb's operand 32 KB on
         auto twiddle = [&](unsigned char *op) {
             unsigned char *opb = op + (N2 == 64 ? 0 : 32768 * rb);
             const int rg0 = N2 == 64 ? 8 * rb : 0;  // row group of m2 = 0
@@ -601,17 +704,17 @@ __global__ void __launch_bounds__(TcShape<LOG2N>::THREADS, TcShape<LOG2N>::CTAS_
                 for (int q = 0; q < 2; ++q) {
                     const int off = (rg0 + 4 * g + 2 * p + q) * 128 + (ri >> 3) * 2048 + (ri & 7) * 16;
                     st_shared_v4(opb + off, pr[4 * q], pr[4 * q + 1], pr[4 * q + 2], pr[4 * q + 3]);
-                    st_shared_v4(opb + off + 8 * 2048, pim[4 * q], pim[4 * q + 1], pim[4 * q + 2], pim[4 * q + 3]);
+                    st_shared_v4(opb + off + S::IM2_OFF, pim[4 * q], pim[4 * q + 1], pim[4 * q + 2], pim[4 * q + 3]);
                 }
             }
         };
 
-        // D2 -> outputs m = M + N2 c + m2 (c = 16 oh + u) of pair i: series,
+        // D2 -> outputs m = M + N2 c + m2 (c = 16 oh + u) of step i: series,
         // detection into the intensity buffers (M floats per block, in `op`)
         auto outputs = [&](int i, unsigned char *op) {
-            const int k = kb + 2 * i;
+            const int k = kb + BPS * i;
             float yr[16], yi[16];
-            tmem_ld_2x16(tD2b + 16 * oh, tD2b + 32 + 16 * oh, yr, yi);
+            tmem_ld_2x16(tD2b + 16 * oh, tD2b + S::D2_HALF + 16 * oh, yr, yi);
             if constexpr (SERIES) {
                 if (ob == 0 || k + 1 < ke) {
                     float2 *out = a.series + (size_t)dm * a.count * M + (size_t)(k + ob) * M + 16 * N2 * oh + om2;
@@ -689,16 +792,19 @@ __global__ void __launch_bounds__(TcShape<LOG2N>::THREADS, TcShape<LOG2N>::CTAS_
                 outputs(i, sm + cur);
                 tc_fence_before();
                 if constexpr (FOLD) {
-                    // the pair's 2M intensities are contiguous: one pass when
-                    // one period span holds them, else block by block
-                    const int k = kb + 2 * i;
+                    // the step's intensities are contiguous: one pass when one
+                    // period span holds them, else unit by unit (a unit: one
+                    // block at 4096 and 8192, half of the block at 16384)
+                    constexpr int FU = BPS == 2 ? M : M / 2;
+                    const int k = kb + BPS * i;
+                    const bool second = BPS == 1 || k + 1 < ke;
                     const float *ib0 = reinterpret_cast<const float *>(sm + cur);
                     __syncthreads();
-                    if (!(k + 1 < ke && fold_pair<kIbufSwizzled>(a.fold, fw, ib0, k * M, M, sp, sbase, scnt))) {
-                        fold_block<kIbufSwizzled>(a.fold, fw, ib0, k * M, M, sp, sbase, scnt);
-                        if (k + 1 < ke) {
+                    if (!(second && fold_pair<kIbufSwizzled>(a.fold, fw, ib0, k * M, FU, sp, sbase, scnt))) {
+                        fold_block<kIbufSwizzled>(a.fold, fw, ib0, k * M, FU, sp, sbase, scnt);
+                        if (second) {
                             __syncthreads();
-                            fold_block<kIbufSwizzled>(a.fold, fw, ib0 + M, (k + 1) * M, M, sp, sbase, scnt);
+                            fold_block<kIbufSwizzled>(a.fold, fw, ib0 + FU, k * M + FU, FU, sp, sbase, scnt);
                         }
                     }
                 }
@@ -757,7 +863,7 @@ __global__ void __launch_bounds__(TcShape<LOG2N>::THREADS, TcShape<LOG2N>::CTAS_
 // One GEMM of the kernel on given data (layout check): A from a row-major
 // 128 x K 16-bit matrix, B the kernel's constant operand, D read back
 // through the kernel's tensor-memory view.  Step 1: GEMM 1 (K = 2 N2,
-// 2 N2 columns), step 2: GEMM 2 (K = 128, 64 columns).
+// 2 N2 columns), step 2: GEMM 2 (K = 2 N1, N1 columns).
 template <int LOG2N>
 __global__ void __launch_bounds__(kThreads, 1) tc_probe_kernel(int step, const uint16_t *A, float *D, int *status)
 {
@@ -766,7 +872,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_probe_kernel(int step, const u
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const uint32_t s0 = smem_addr(sm);
     const uint32_t bar = s0 + S::SMEM_CTL;
-    const int kdim = step == 1 ? 2 * S::N2 : 128;
+    const int kdim = step == 1 ? 2 * S::N2 : 2 * S::N1;
     fill_constants<F16, LOG2N>(sm, tid);
     for (int e = tid; e < 128 * kdim; e += blockDim.x) {
         const int r = e & 127, kk = e >> 7;
@@ -776,11 +882,15 @@ __global__ void __launch_bounds__(kThreads, 1) tc_probe_kernel(int step, const u
     const uint32_t tcol = step == 1 ? 0u : (uint32_t)S::D2_COL;
     if (tid == 0) {
         tc_fence_after();
-        if (step == 1)
+        if (step == 1) {
             issue_cgemm<F16>(tmem, s0 + S::SMEM_OP0, s0 + S::SMEM_B1, S::N2, S::N2 / 16, S::SBO_B1);
-        else
+            mma_commit(bar);
+        } else if constexpr (S::N1 == 128) {
+            issue_gemm2<F16, LOG2N>(tmem, s0, s0 + S::SMEM_OP0, bar);
+        } else {
             issue_cgemm<F16>(tmem + tcol, s0 + S::SMEM_OP0, s0 + S::SMEM_B2, 32, 4, 1024);
-        mma_commit(bar);
+            mma_commit(bar);
+        }
     }
     uint32_t parity = 0;
     if (!wait_gemm(tid, bar, parity)) {
@@ -791,7 +901,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_probe_kernel(int step, const u
         tc_teardown<LOG2N>(tmem, warp);
         return;
     }
-    const int ncol = step == 1 ? 2 * S::N2 : 64;
+    const int ncol = step == 1 ? 2 * S::N2 : 2 * S::D2_HALF;
     const int row = 32 * (warp & 3) + lane, h = warp >> 2;
     const uint32_t base = tmem + tcol + ((uint32_t)(32 * (warp & 3)) << 16);
     for (int c0 = h * ncol / 2; c0 < (h + 1) * ncol / 2; c0 += 32) {
@@ -886,14 +996,18 @@ cudaError_t launch_tc_t(bool bf16, bool series, bool fold, const DedispArgs &a, 
 
 bool tc_supported(int log2n) { return log2n >= kLog2NMin && log2n <= kLog2NMax; }
 
-int tc_threads(int log2n) { return log2n == 13 ? TcShape<13>::THREADS : TcShape<12>::THREADS; }
+int tc_threads(int log2n) { return log2n == 12 ? TcShape<12>::THREADS : TcShape<13>::THREADS; }
+
+int tc_blocks_per_step(int log2n) { return log2n == 14 ? TcShape<14>::BPS : TcShape<12>::BPS; }
 
 // Resident CTAs per SM from the shared-memory and register limits (the
-// tensor memory allows two at N = 4096, one at N = 8192); 0 when it does not
-// fit.  The occupancy API is not used: it reports one CTA per SM for the
+// tensor memory allows two at N = 4096, one at N = 8192 and 16384); 0 when it
+// does not fit.  The occupancy API is not used: it reports one CTA per SM for the
 // 4096-point kernel where the hardware runs two.
 int tc_blocks_per_sm(int log2n, bool bf16, bool series, bool fold, size_t extra_smem)
 {
+    if (log2n == 14)
+        return tc_blocks_per_sm_t<14>(bf16, series, fold, extra_smem);
     if (log2n == 13)
         return tc_blocks_per_sm_t<13>(bf16, series, fold, extra_smem);
     return tc_blocks_per_sm_t<12>(bf16, series, fold, extra_smem);
@@ -907,6 +1021,8 @@ cudaError_t launch_tc_dedisp(int log2n, bool bf16, bool series, bool fold, const
     const NoBatch none{};
     const size_t fs = fold ? fold_smem_bytes(a.fold.nbins, a.fold.span_cap, a.fold.smem_prof != 0, tc_threads(log2n))
                            : 0;
+    if (log2n == 14)
+        return launch_tc_t<14, false>(bf16, series, fold, a, none, fs, grid, st);
     if (log2n == 13)
         return launch_tc_t<13, false>(bf16, series, fold, a, none, fs, grid, st);
     return launch_tc_t<12, false>(bf16, series, fold, a, none, fs, grid, st);
@@ -918,6 +1034,8 @@ cudaError_t launch_tc_dedisp_batch(int log2n, bool bf16, bool series, bool fold,
     if (!b.counter || b.nobs < 1 || b.nobs > kBatchMax || !tc_supported(log2n))
         return cudaErrorInvalidValue;
     DedispArgs none{};
+    if (log2n == 14)
+        return launch_tc_t<14, true>(bf16, series, fold, none, b, fold_smem, grid, st);
     if (log2n == 13)
         return launch_tc_t<13, true>(bf16, series, fold, none, b, fold_smem, grid, st);
     return launch_tc_t<12, true>(bf16, series, fold, none, b, fold_smem, grid, st);
@@ -932,8 +1050,9 @@ cudaError_t launch_tc_permute_rows(const float2 *in, float2 *out, int rows, int 
 
 cudaError_t launch_tc_probe(int step, const uint16_t *a, float *d, int *status, cudaStream_t st)
 {
-    // steps 1, 2: the 4096-point GEMMs; step 3: the 8192-point GEMM 1
-    if (step < 1 || step > 3)
+    // steps 1, 2: the 4096-point GEMMs; step 3: the 8192-point GEMM 1 (also
+    // the 16384-point GEMM 1); step 4: the 16384-point GEMM 2
+    if (step < 1 || step > 4)
         return cudaErrorInvalidValue;
     auto run = [&](auto k, size_t sm, int st_) -> cudaError_t {
         cudaError_t e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
@@ -942,6 +1061,8 @@ cudaError_t launch_tc_probe(int step, const uint16_t *a, float *d, int *status, 
         k<<<1, kThreads, sm, st>>>(st_, a, d, status);
         return cudaGetLastError();
     };
+    if (step == 4)
+        return run(tc_probe_kernel<14>, (size_t)TcShape<14>::SMEM_FOLD, 2);
     if (step == 3)
         return run(tc_probe_kernel<13>, (size_t)TcShape<13>::SMEM_FOLD, 1);
     return run(tc_probe_kernel<12>, (size_t)TcShape<12>::SMEM_FOLD, step);

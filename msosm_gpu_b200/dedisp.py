@@ -71,7 +71,8 @@ class Dedisperser:
     dedispersed series (needed by get_output); ``osm`` selects classical
     overlap-save.  ``precision`` "fp32" (default) runs the inverse transforms
     on the CUDA cores in FP32; "fp16" / "bf16" run them on the tensor cores
-    with f16 / bf16 operands and f32 accumulation (FFT sizes 4096 and 8192).
+    with f16 / bf16 operands and f32 accumulation (FFT sizes 4096, 8192 and
+    16384).
     """
 
     def __init__(self, bw, dm, f0, fftpoint: int = 0, count: int = 1, input_size: int = 0,
@@ -403,12 +404,13 @@ def tc_gemm_check(step: int, a: np.ndarray) -> np.ndarray:
     """Run GEMM ``step`` of the tensor-core kernel on a float16 matrix ``a``
     with the kernel's own layouts (msosm_tc_gemm_check): steps 1, 2 the
     4096-point GEMMs (a 128 x 128; result 128 x 128 / 128 x 64), step 3 the
-    8192-point GEMM 1 (a 128 x 256; result 128 x 256).  Returns a @ B_step
+    8192- and 16384-point GEMM 1 (a 128 x 256; result 128 x 256), step 4 the
+    16384-point GEMM 2 (a 128 x 256; result 128 x 128).  Returns a @ B_step
     as float32."""
     a = np.ascontiguousarray(a, dtype=np.float16)
-    kdim = 256 if step == 3 else 128
+    kdim = 256 if step >= 3 else 128
     if a.shape != (128, kdim):
         raise ValueError(f"a must be 128 x {kdim}")
-    d = np.zeros((128, {1: 128, 2: 64, 3: 256}[step]), np.float32)
+    d = np.zeros((128, {1: 128, 2: 64, 3: 256, 4: 128}[step]), np.float32)
     check(lib().msosm_tc_gemm_check(int(step), a.view(np.uint16).ctypes.data, d.ctypes.data))
     return d

@@ -21,15 +21,17 @@ def test_candidates_respect_minimum_and_budget():
     assert any(p == "bf16" for _, p in A.candidates(16e6, dms, 1242e6, budget=5e-3))
     assert [p for _, p in A.candidates(16e6, dms, 1242e6, budget=1e-5)] == ["fp32"] * len(
         {n for n, _ in c})
-    # a long smear leaves no tensor candidate
+    # a long smear leaves the tensor cores only their largest size, 16384
     big = A.candidates(64e6, [300.0], 1068e6)
-    assert all(p == "fp32" and n >= 16384 for n, p in big)
+    assert all(n >= 16384 for n, _ in big) and any(n > 16384 for n, _ in big)
+    assert {n for n, p in big if p != "fp32"} == {16384}
 
 
 def test_fixed_choice():
     assert A.fixed_choice(16e6, [50.0], 1242e6, 4096, "fp16") == (4096, "fp16")
-    n, p = A.fixed_choice(64e6, [300.0], 1068e6, 4096, "fp16")
-    assert n >= 16384 and p == "fp32"
+    assert A.fixed_choice(64e6, [300.0], 1068e6, 4096, "fp16") == (16384, "fp16")
+    # above the tensor path's sizes the fixed choice falls back to FP32
+    assert A.fixed_choice(64e6, [300.0], 1068e6, 32768, "fp16") == (32768, "fp32")
     assert A.fixed_choice(16e6, [1.0], 1242e6, 2048, "fp32") == (2048, "fp32")
 
 

@@ -1,6 +1,6 @@
 """Many observations in one launch (msosm_batch / DedispBatch): observations
-of different length, band, trial grid and FFT size dedispersed by one
-persistent tensor-core launch per kernel group, every observation's series
+of different length, band, trial grid and FFT size (4096, 8192, 16384)
+dedispersed by one persistent tensor-core launch per kernel group, every observation's series
 and folded profiles against the FP64 oracle (the tensor path's bounds) and
 against the same observation run through its own handle (the batch keeps
 each handle's own work items, so the two agree to rounding).  An FP32 handle in
@@ -21,6 +21,7 @@ OBS = [  # bw, f0, dms, fftpoint, count, precision, period (smears short enough 
     (32e6, 1384e6, [1.0, 4.0, 6.0, 8.0], 4096, 12, "fp16", 0.00045),
     (16e6, 1242e6, [2.0, 9.0], 4096, 9, "fp16", 0.00029),
     (4e6, 1098e6, [3.0, 30.0], 2048, 6, "fp32", 0.0013),
+    (16e6, 1242e6, [1.0, 5.0], 16384, 3, "fp16", 0.0011),
 ]
 
 
@@ -42,7 +43,7 @@ def test_batch_matches_oracle_and_own_handles():
     solo_h = [make(o) for o in OBS]
     b = DedispBatch(batch_h)
     info = b.info()
-    assert info["groups"] == 2 and info["launches_per_call"] == 3
+    assert info["groups"] == 3 and info["launches_per_call"] == 4
     orc = [O.Dedisp(o[0], o[2], o[1], o[3], o[4]) for o in OBS]
     folds = [[O.Fold(o[6], o[0], d.block_samples, 64) for _ in o[2]] for o, d in zip(OBS, batch_h)]
     for fl, d in zip(folds, batch_h):

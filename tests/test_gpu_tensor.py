@@ -33,20 +33,21 @@ def rel_rms(a, b):
 def dft_operand(step):
     """The real form of the inverse DFT the kernel multiplies by, K x N with
     K = [Re | Im] of the input index, rounded to float16: step 1 the 64-point
-    DFT, step 2 its frequencies 32..63, step 3 the 128-point DFT."""
-    p = 128 if step == 3 else 64
+    DFT, step 2 its frequencies 32..63, step 3 the 128-point DFT, step 4 its
+    frequencies 64..127 (FFT 16384's second GEMM)."""
+    p = 128 if step >= 3 else 64
     k = np.arange(p)[:, None]
-    m = np.arange(32, 64)[None, :] if step == 2 else np.arange(p)[None, :]
+    m = {2: np.arange(32, 64), 4: np.arange(64, 128)}.get(step, np.arange(p))[None, :]
     ang = 2 * np.pi * ((k * m) % p) / p
     c, s = np.cos(ang), np.sin(ang)
     B = np.block([[c, s], [-s, c]])
     return B.astype(np.float16).astype(np.float64)
 
 
-@pytest.mark.parametrize("step", [1, 2, 3])
+@pytest.mark.parametrize("step", [1, 2, 3, 4])
 def test_gemm_layout_and_readback(step):
     rng = np.random.default_rng(step)
-    a = rng.standard_normal((128, 256 if step == 3 else 128)).astype(np.float16)
+    a = rng.standard_normal((128, 256 if step >= 3 else 128)).astype(np.float16)
     d = tc_gemm_check(step, a)
     ref = a.astype(np.float64) @ dft_operand(step)
     err = np.max(np.abs(d - ref)) / np.max(np.abs(ref))
@@ -97,6 +98,35 @@ def test_series_8192_matches_oracle(count, calls, precision):
         assert e < TOL[precision][0], (dms[i], e)
 
 
+@pytest.mark.parametrize("precision", ["fp16", "bf16"])
+@pytest.mark.parametrize("count,calls", [(3, 3), (2, 4), (1, 4)])
+def test_series_16384_matches_oracle(count, calls, precision):
+    # the 16384-point shape: 128 x 128 factorisation, one block per step
+    # (both halves of its row), GEMM 2's constant from GEMM 1's columns
+    dms = [0.0, 5.0, 60.0, 200.0]
+    ours, ref, d, _ = run_pair(dms, count, calls, seed=50 + count, precision=precision, fft=16384)
+    assert d.fftpoint == 16384
+    for i in range(len(dms)):
+        e = rel_rms(ours[i], ref[i])
+        assert e < TOL[precision][0], (dms[i], e)
+
+
+@pytest.mark.parametrize("fft", [8192, 16384])
+def test_series_matches_fp32_path_large(fft):
+    dms = list(np.linspace(0, 150, 12))
+    count, calls = 65536 // fft, 3
+    t = Dedisperser(BW, dms, F0, fft, count, precision="fp16")
+    f = Dedisperser(BW, dms, F0, fft, count)
+    x = u16(t.block_samples * calls, 12)
+    for c in range(calls):
+        blk = x[c * t.block_samples:(c + 1) * t.block_samples]
+        t.filter_block(blk)
+        f.filter_block(blk)
+        a, b = t.get_output(), f.get_output()
+        for i in range(len(dms)):
+            assert rel_rms(a[i], b[i]) < SERIES_TOL
+
+
 def test_series_matches_fp32_path():
     dms = list(np.linspace(0, 100, 16))
     count, calls = 8, 3
@@ -141,7 +171,7 @@ def test_full_scale_tone_stays_finite_and_accurate():
         assert rel_rms(ours[i], ref[i]) < SERIES_TOL
 
 
-@pytest.mark.parametrize("precision,fft", [("fp16", 4096), ("bf16", 4096), ("fp16", 8192)])
+@pytest.mark.parametrize("precision,fft", [("fp16", 4096), ("bf16", 4096), ("fp16", 8192), ("fp16", 16384)])
 def test_fold_matches_oracle(precision, fft):
     dms, count, calls, period, tb = [0.0, 20.0, 73.2], 8 * 4096 // fft, 6, 0.0011, 256
     d = Dedisperser(BW, dms, F0, fft, count, series=False, precision=precision)
@@ -167,7 +197,8 @@ def test_fold_matches_oracle(precision, fft):
 
 
 @pytest.mark.parametrize("precision,fft,detect", [("fp16", 4096, "power"), ("fp16", 8192, "power"),
-                                                  ("fp16", 4096, "amplitude"), ("bf16", 8192, "power")])
+                                                  ("fp16", 4096, "amplitude"), ("bf16", 8192, "power"),
+                                                  ("fp16", 16384, "power"), ("fp16", 16384, "amplitude")])
 def test_series_and_fold_in_one_pass(precision, fft, detect):
     # the kernel that writes the series and folds in the same pass: both
     # outputs against the oracle, |y| as well as |y|^2 detection
@@ -212,7 +243,7 @@ def test_complex64_device_input_matches_uint16_host_input():
         assert np.array_equal(a.get_output(), b.get_output())
 
 
-@pytest.mark.parametrize("fftpoint", [4096, 8192])
+@pytest.mark.parametrize("fftpoint", [4096, 8192, 16384])
 def test_wait_timeout_reports_and_handle_recovers(fftpoint):
     # a wait limit of 0 makes the kernel's first wait on a GEMM give up: it
     # takes its timeout exit (status word, drain of its own GEMMs, tensor
