@@ -176,6 +176,51 @@ __device__ __forceinline__ void tmem_ld_2x16(uint32_t ta, uint32_t tb, float (&a
     }
 }
 
+// 32 words of this thread's TMEM lane, columns ta .. ta + 31 (two x16 stores), then the wait
+__device__ __forceinline__ void tmem_st_32(uint32_t ta, const uint32_t (&v)[32])
+{
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17};\n\t"
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%1], {%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32,%33};\n\t"
+        "tcgen05.wait::st.sync.aligned;" ::"r"(ta), "r"(ta + 16),
+        "r"(v[0]), "r"(v[1]), "r"(v[2]), "r"(v[3]), "r"(v[4]), "r"(v[5]), "r"(v[6]), "r"(v[7]), "r"(v[8]), "r"(v[9]),
+        "r"(v[10]), "r"(v[11]), "r"(v[12]), "r"(v[13]), "r"(v[14]), "r"(v[15]), "r"(v[16]), "r"(v[17]), "r"(v[18]),
+        "r"(v[19]), "r"(v[20]), "r"(v[21]), "r"(v[22]), "r"(v[23]), "r"(v[24]), "r"(v[25]), "r"(v[26]), "r"(v[27]),
+        "r"(v[28]), "r"(v[29]), "r"(v[30]), "r"(v[31])
+        : "memory");
+}
+
+// D1 re / im (x16 each) and 8 + 8 twiddle words (x8 each), one wait
+__device__ __forceinline__ void tmem_ld_twiddle(uint32_t ta, uint32_t tb, uint32_t tc, uint32_t td, float (&a)[16],
+                                                float (&b)[16], uint32_t (&c)[8], uint32_t (&d)[8])
+{
+    uint32_t r[48];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%48];\n\t"
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%49];\n\t"
+        "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%32,%33,%34,%35,%36,%37,%38,%39}, [%50];\n\t"
+        "tcgen05.ld.sync.aligned.32x32b.x8.b32 {%40,%41,%42,%43,%44,%45,%46,%47}, [%51];\n\t"
+        "tcgen05.wait::ld.sync.aligned;"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
+          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]),
+          "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]),
+          "=r"(r[40]), "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47])
+        : "r"(ta), "r"(tb), "r"(tc), "r"(td)
+        : "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+        a[i] = __uint_as_float(r[i]);
+        b[i] = __uint_as_float(r[16 + i]);
+    }
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        c[i] = r[32 + i];
+        d[i] = r[40 + i];
+    }
+}
+
 // The 16-bit operand type: f16 (scaled into range) or bf16.
 struct F16 {
     using h1 = __half;
@@ -422,6 +467,25 @@ __global__ void __launch_bounds__(TcShape<LOG2N>::THREADS, TcShape<LOG2N>::CTAS_
         sincospif((float)((ri * (m2 + 1)) & (N - 1)) * (2.0f / N), &s1f, &c1f);
         twr[i] = E::pack(c0f, c1f);
         twi[i] = E::pack(s0f, s1f);
+    }
+    // At N = 16384, and in the batch kernel, the twiddles wait in this
+    // thread's tensor-memory lane (columns past D2, 32 per column group g)
+    // and are read with D1 in each twiddle pass: the 32 registers go to the
+    // gather, which at 16384 also holds the filter values it reads each step
+    // (29.3 vs 33.4 ms per 2^24 samples x 256 trials), and in the batch
+    // kernel to the parameter-table reads (spills 20/20 instead of 152/272
+    // bytes; 1-3 % faster).  In the one-handle kernel at 4096 and 8192 the
+    // extra tensor-memory read in the twiddle pass cost 8-11 %.
+    constexpr bool kTwInTmem = LOG2N == 14 || MULTI;
+    const uint32_t tTW = tmem + lane_base + (uint32_t)(S::TW_COL + 32 * g);
+    if constexpr (kTwInTmem) {
+        uint32_t v[32];
+#pragma unroll
+        for (int i = 0; i < 16; ++i) {
+            v[i] = *reinterpret_cast<const uint32_t *>(&twr[i]);
+            v[16 + i] = *reinterpret_cast<const uint32_t *>(&twi[i]);
+        }
+        tmem_st_32(tTW, v);
     }
 
     uint32_t phA = 0, phB = 0;
@@ -688,13 +752,21 @@ __global__ void __launch_bounds__(TcShape<LOG2N>::THREADS, TcShape<LOG2N>::CTAS_
 #pragma unroll
             for (int p = 0; p < 2; ++p) {
                 float re[16], im[16];
-                tmem_ld_2x16(tD1 + 32 * g + 16 * p, tD1 + N2 + 32 * g + 16 * p, re, im);
+                uint32_t w8r[8], w8i[8];
+                if constexpr (kTwInTmem)
+                    tmem_ld_twiddle(tD1 + 32 * g + 16 * p, tD1 + N2 + 32 * g + 16 * p, tTW + 8 * p, tTW + 16 + 8 * p,
+                                    re, im, w8r, w8i);
+                else
+                    tmem_ld_2x16(tD1 + 32 * g + 16 * p, tD1 + N2 + 32 * g + 16 * p, re, im);
                 uint32_t pr[8], pim[8];
 #pragma unroll
                 for (int i = 0; i < 8; ++i) {
                     const typename E::h2 ar = E::pack(re[2 * i], re[2 * i + 1]);
                     const typename E::h2 ai = E::pack(im[2 * i], im[2 * i + 1]);
-                    const typename E::h2 wr = twr[8 * p + i], wi = twi[8 * p + i];
+                    const typename E::h2 wr =
+                        kTwInTmem ? *reinterpret_cast<const typename E::h2 *>(&w8r[i]) : twr[8 * p + i];
+                    const typename E::h2 wi =
+                        kTwInTmem ? *reinterpret_cast<const typename E::h2 *>(&w8i[i]) : twi[8 * p + i];
                     const typename E::h2 orr = __hfma2(ar, wr, __hneg2(__hmul2(ai, wi)));
                     const typename E::h2 oi = __hfma2(ar, wi, __hmul2(ai, wr));
                     pr[i] = *reinterpret_cast<const uint32_t *>(&orr);

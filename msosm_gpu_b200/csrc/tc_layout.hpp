@@ -62,6 +62,7 @@ struct TcShape {
     static constexpr int IM2_OFF = (N1 / 8) * 2048;        // GEMM 2 operand: Im part, K = N1 on
     static constexpr int D2_COL = 2 * N2;                  // TMEM: D1 at 0 .. 2 N2 - 1, D2 after it
     static constexpr int D2_HALF = N1 / 2;                 // D2 columns per part (Re, Im) of one block
+    static constexpr int TW_COL = D2_COL + (N2 == 64 ? 64 : 128);  // past D2: 32 spare columns per column group
     static constexpr int TMEM_COLS = LOG2N == 12 ? 256 : 512;
     static constexpr int SCALE_EXP = LOG2N == 12 ? 8 : 7;  // |Z| < 2^SCALE_EXP: GEMM 1 sums < 2^15
 };
