@@ -59,6 +59,7 @@ def ours(dms, fftpoint, count, x_u16, calls, osm=False, precision="fp32"):
     (1024, 4, [1.0, 3.5, 7.0]),
     (4096, 8, [25.0, 50.0, 73.2, 100.0]),
     (8192, 2, [150.0]),
+    (16384, 2, [60.0, 300.0]),
 ])
 def test_concurrent_matches_reference_gpu(fftpoint, count, dms):
     calls = 6
@@ -73,7 +74,8 @@ def test_concurrent_matches_reference_gpu(fftpoint, count, dms):
         assert rel_rms(y[i], ref[i]) < RTOL, (i, rel_rms(y[i], ref[i]))
 
 
-@pytest.mark.parametrize("fftpoint,count,dms", [(4096, 8, [0.5, 50.0, 73.2, 100.0]), (8192, 4, [150.0, 200.0])])
+@pytest.mark.parametrize("fftpoint,count,dms", [(4096, 8, [0.5, 50.0, 73.2, 100.0]), (8192, 4, [150.0, 200.0]),
+                                                (16384, 2, [0.5, 90.0, 300.0])])
 def test_tensor_core_path_matches_reference_gpu(fftpoint, count, dms):
     # the f16 tensor-core path against the reference's cuFFT path on the
     # same input, within the tensor path's stated series error (1.5e-3)
