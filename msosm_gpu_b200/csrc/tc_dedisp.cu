@@ -627,8 +627,8 @@ __global__ void __launch_bounds__(TcShape<LOG2N>::THREADS, TcShape<LOG2N>::CTAS_
                 if (kg >= a.max_delay) {
                     // as the pair gather below, over the two row halves of
                     // one block in turn, with the filter read alongside the
-                    // ring (both halves' loads in flight at once spilled
-                    // twice as much and took 21 % longer)
+                    // ring (both halves' loads in flight at once took 7 %
+                    // longer, 21 % with the twiddles in registers)
 #pragma unroll
                     for (int h = 0; h < 2; ++h) {
                         float4 xa[8], hv[8];
