@@ -43,8 +43,10 @@ namespace {
 using namespace tc;
 
 constexpr unsigned long long kWaitLimitNs = 1000000000ull;
-// try_wait sleeps up to this long (or until the phase completes) per attempt
-constexpr uint32_t kSuspendHintNs = 100000u;
+// Wait limits below this probe without suspending (test_wait); longer ones
+// use try_wait, which suspends for the hardware's own time limit per
+// attempt (an explicit 100 us suspend hint was 0.4-0.8 % slower)
+constexpr unsigned long long kProbeBelowNs = 100000ull;
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -63,10 +65,10 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity)
     uint32_t ok;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2, %3;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
         "selp.u32 %0, 1, 0, p;\n\t}"
         : "=r"(ok)
-        : "r"(bar), "r"(parity), "r"(kSuspendHintNs)
+        : "r"(bar), "r"(parity)
         : "memory");
     return ok != 0;
 }
@@ -93,7 +95,7 @@ __device__ __forceinline__ bool mbar_test_wait(uint32_t bar, uint32_t parity)
 }
 
 // Waits for the phase of the given parity to complete; false after limit_ns.
-// A limit below the suspend hint probes without suspending; a limit of 0
+// A limit below kProbeBelowNs probes without suspending; a limit of 0
 // gives up at once, without probing (a diagnostic setting: the kernel then
 // takes its timeout exit, whose drain of the GEMMs in flight keeps its own
 // limit).
@@ -101,7 +103,7 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, unsigne
 {
     if (limit_ns == 0)
         return false;
-    if (limit_ns < kSuspendHintNs) {
+    if (limit_ns < kProbeBelowNs) {
         if (mbar_test_wait(bar, parity))
             return true;
         const unsigned long long t0 = global_ns();
