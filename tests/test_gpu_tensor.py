@@ -196,6 +196,35 @@ def test_fold_matches_oracle(precision, fft):
         assert e < TOL[precision][1], (dms[i], e)
 
 
+@pytest.mark.parametrize("fft", [8192, 16384])
+def test_fold_many_short_bins_in_global_rows(fft):
+    # 4096 bins of 4 samples: above the 2048 bins these kernels keep in
+    # shared memory (the work items' partial rows live in global memory) and
+    # below the 16 samples per bin of the one-pass fast path (each block goes
+    # span piece by span piece)
+    dms, count, calls, period, tb = [0.0, 30.0], 65536 // fft, 4, 0.0011, 4096
+    d = Dedisperser(BW, dms, F0, fft, count, series=False, precision="fp16")
+    nd = 4096
+    d.fold_init(period, BW, time_bin=tb, discard_Nd=nd)
+    o = O.Dedisp(BW, dms, F0, fft, count)
+    x = u16(d.block_samples * calls, 27)
+    ser = []
+    for c in range(calls):
+        blk = x[c * d.block_samples:(c + 1) * d.block_samples]
+        d.filter_block(blk)
+        ser.append(o.filter(O.decode_uint16(blk)))
+    ser = np.concatenate(ser, 1)
+    prof = d.get_profiles()
+    assert prof.shape == (len(dms), tb) and d.folded_periods() > 0
+    for i in range(len(dms)):
+        f = O.Fold(period, BW, d.block_samples, tb)
+        f.discard_samples(nd)
+        for c in range(calls):
+            f.fold_data(np.abs(ser[i, c * d.block_samples:(c + 1) * d.block_samples]) ** 2)
+        # 4 samples per bin average little: the bound is the series one
+        assert rel_rms(prof[i], f.fold_data_bins()) < SERIES_TOL, dms[i]
+
+
 @pytest.mark.parametrize("precision,fft,detect", [("fp16", 4096, "power"), ("fp16", 8192, "power"),
                                                   ("fp16", 4096, "amplitude"), ("bf16", 8192, "power"),
                                                   ("fp16", 16384, "power"), ("fp16", 16384, "amplitude")])
