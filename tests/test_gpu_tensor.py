@@ -196,13 +196,15 @@ def test_fold_matches_oracle(precision, fft):
         assert e < TOL[precision][1], (dms[i], e)
 
 
-@pytest.mark.parametrize("fft", [8192, 16384])
-def test_fold_many_short_bins_in_global_rows(fft):
-    # 4096 bins of 4 samples: above the 2048 bins these kernels keep in
-    # shared memory (the work items' partial rows live in global memory) and
-    # below the 16 samples per bin of the one-pass fast path (each block goes
-    # span piece by span piece)
-    dms, count, calls, period, tb = [0.0, 30.0], 65536 // fft, 4, 0.0011, 4096
+@pytest.mark.parametrize("fft,period,tb", [(8192, 0.0011, 4096), (16384, 0.0011, 4096), (4096, 0.0008, 1024),
+                                           (16384, 0.0008, 1024)])
+def test_fold_short_bins(fft, period, tb):
+    # 4096 bins of 4 samples: above the 2048 bins the 8192 and 16384 kernels
+    # keep in shared memory (the work items' partial rows live in global
+    # memory) and below 8 samples per bin (each block goes span piece by span
+    # piece); 1024 bins of 12 samples: the 8-samples-per-thread fast path of
+    # a block instead of the one-pass fold of a step (>= 16 samples per bin)
+    dms, count, calls = [0.0, 30.0], 65536 // fft, 4
     d = Dedisperser(BW, dms, F0, fft, count, series=False, precision="fp16")
     nd = 4096
     d.fold_init(period, BW, time_bin=tb, discard_Nd=nd)
@@ -221,7 +223,7 @@ def test_fold_many_short_bins_in_global_rows(fft):
         f.discard_samples(nd)
         for c in range(calls):
             f.fold_data(np.abs(ser[i, c * d.block_samples:(c + 1) * d.block_samples]) ** 2)
-        # 4 samples per bin average little: the bound is the series one
+        # 4 or 12 samples per bin average little: the bound is the series one
         assert rel_rms(prof[i], f.fold_data_bins()) < SERIES_TOL, dms[i]
 
 
