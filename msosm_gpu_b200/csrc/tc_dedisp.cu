@@ -330,16 +330,19 @@ __device__ __forceinline__ void issue_cgemm(uint32_t tmem_d, uint32_t a, uint32_
     const uint32_t id_full = idesc_f16(128, 2 * half, true, false, E::fmt);
     const uint32_t id_neg = idesc_f16(128, half, true, true, E::fmt);
     const uint32_t id_half = idesc_f16(128, half, true, false, E::fmt);
+    // descriptors built once; a K step moves only the 14-bit start field
+    // (addresses stay below 256 KB, so the field never carries).  Thread 0
+    // issues every MMA while the CTA waits at its next barrier: rebuilding
+    // both descriptors per MMA cost 0.6-1.1 % of the kernel
+    const uint64_t da = smem_desc(a, 2048, 128), db = smem_desc(b, 128, sbo);
+    const uint64_t dbs = smem_desc(b + (uint32_t)(half >> 3) * sbo, 128, sbo);
+    const uint64_t sa = kDescStepA >> 4, sb = kDescStepB >> 4;
     for (int s = 0; s < ksteps; ++s)
-        mma_f16(tmem_d, smem_desc(a + s * kDescStepA, 2048, 128), smem_desc(b + s * kDescStepB, 128, sbo), id_full,
-                s > 0 ? 1u : 0u);
-    const uint32_t bs = b + (uint32_t)(half >> 3) * sbo;
+        mma_f16(tmem_d, da + s * sa, db + s * sb, id_full, s > 0 ? 1u : 0u);
     for (int s = 0; s < ksteps; ++s)
-        mma_f16(tmem_d, smem_desc(a + (ksteps + s) * kDescStepA, 2048, 128),
-                smem_desc(bs + s * kDescStepB, 128, sbo), id_neg, 1u);
+        mma_f16(tmem_d, da + (ksteps + s) * sa, dbs + s * sb, id_neg, 1u);
     for (int s = 0; s < ksteps; ++s)
-        mma_f16(tmem_d + half, smem_desc(a + (ksteps + s) * kDescStepA, 2048, 128),
-                smem_desc(b + s * kDescStepB, 128, sbo), id_half, 1u);
+        mma_f16(tmem_d + half, da + (ksteps + s) * sa, db + s * sb, id_half, 1u);
 }
 
 // The same complex GEMM with C and S at separate places (bc, bs; N = half
@@ -350,18 +353,16 @@ __device__ __forceinline__ void issue_cgemm_cs(uint32_t tmem_d, uint32_t a, uint
 {
     const uint32_t id_neg = idesc_f16(128, half, true, true, E::fmt);
     const uint32_t id_half = idesc_f16(128, half, true, false, E::fmt);
+    const uint64_t da = smem_desc(a, 2048, 128), dc = smem_desc(bc, 128, sbo), ds = smem_desc(bs, 128, sbo);
+    const uint64_t sa = kDescStepA >> 4, sb = kDescStepB >> 4;
     for (int s = 0; s < ksteps; ++s)
-        mma_f16(tmem_d, smem_desc(a + s * kDescStepA, 2048, 128), smem_desc(bc + s * kDescStepB, 128, sbo), id_half,
-                s > 0 ? 1u : 0u);
+        mma_f16(tmem_d, da + s * sa, dc + s * sb, id_half, s > 0 ? 1u : 0u);
     for (int s = 0; s < ksteps; ++s)
-        mma_f16(tmem_d + half, smem_desc(a + s * kDescStepA, 2048, 128), smem_desc(bs + s * kDescStepB, 128, sbo),
-                id_half, s > 0 ? 1u : 0u);
+        mma_f16(tmem_d + half, da + s * sa, ds + s * sb, id_half, s > 0 ? 1u : 0u);
     for (int s = 0; s < ksteps; ++s)
-        mma_f16(tmem_d, smem_desc(a + (ksteps + s) * kDescStepA, 2048, 128),
-                smem_desc(bs + s * kDescStepB, 128, sbo), id_neg, 1u);
+        mma_f16(tmem_d, da + (ksteps + s) * sa, ds + s * sb, id_neg, 1u);
     for (int s = 0; s < ksteps; ++s)
-        mma_f16(tmem_d + half, smem_desc(a + (ksteps + s) * kDescStepA, 2048, 128),
-                smem_desc(bc + s * kDescStepB, 128, sbo), id_half, 1u);
+        mma_f16(tmem_d + half, da + (ksteps + s) * sa, dc + s * sb, id_half, 1u);
 }
 
 // GEMM 1 of a step (operand buffer at a), committed to bar
