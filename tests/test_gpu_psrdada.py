@@ -66,6 +66,25 @@ def test_psrdada_two_pol_fold_matches_oracle(tmp_path, blank_reads):
     assert st["reads"] == 40 and st["samples"] == 40 * 4096
 
 
+@pytest.mark.parametrize("fftpoint", [4096, 16384])
+def test_psrdada_two_pol_fold_on_tensor_cores(tmp_path, fftpoint):
+    # the same pipeline with both polarisations' inverse transforms on the
+    # tensor cores (f16 operands): the folded two-pol amplitude profile
+    # within the tensor path's profile bound (1e-4) of the FP64 oracle
+    dm, period, tb = 5.0, 0.0011, 64
+    bw, f0 = BW_MHZ * 1e6, (FREQ_MHZ - BW_MHZ / 2) * 1e6
+    n = 8192 * 20
+    xa = S.pulsar_baseband(n, bw, f0, dm, period, 0.05, 3.0, seed=5)
+    xb = S.pulsar_baseband(n, bw, f0, dm, period, 0.05, 3.0, seed=6)
+    path = str(tmp_path / "tc.dada")
+    P.write_dada(path, S.quantise_uint16(xa, 300.0), S.quantise_uint16(xb, 300.0), BW_MHZ, FREQ_MHZ)
+    ours = P.fold_file(path, dm, period, fftpoint=fftpoint, time_bin=tb, precision="fp16", write=False)
+    ref = oracle_fold(path, dm, period, fftpoint, tb)
+    assert ours.shape == (tb,) and np.any(ours)
+    err = float(np.sqrt(np.mean((ours - ref) ** 2) / np.mean(ref ** 2)))
+    assert err < 1e-4, err
+
+
 def test_psrdada_streaming_reads(tmp_path):
     """Many reads with count > 1 (several FFT blocks per read): the
     overlapped reader keeps order and covers the whole file."""
