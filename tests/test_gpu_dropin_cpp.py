@@ -81,6 +81,47 @@ def test_dropin_classes_match_python_binding():
 
 
 @pytest.mark.gpu
+@pytest.mark.parametrize("fftpoint", [4096, 8192, 16384])
+def test_dropin_classes_on_tensor_cores(fftpoint):
+    # use_tensor_cores(true) before the reference's classes are initialised:
+    # the driver's series equal the Python binding's f16 path bit for bit
+    # and match the FP64 oracle within the tensor path's series bound
+    import oracle as O
+    calls, count = 3, 2
+    blk = count * fftpoint // 2
+    rng = np.random.default_rng(22)
+    x = np.clip(np.rint(rng.standard_normal((blk * calls, 2)) * 1000) + 32768, 1, 65535).astype(np.uint16)
+    src = os.path.join(ROOT, "tests", "cpp", "dropin_tensor_demo.cpp")
+    with tempfile.TemporaryDirectory() as td:
+        exe = os.path.join(td, "demo")
+        subprocess.run(["g++", "-std=c++17", "-O2", "-Wall", "-I", os.path.join(ROOT, "include"), "-o", exe, src,
+                        "-L", LIBDIR, "-lmsosm_b200", f"-Wl,-rpath,{LIBDIR}"], check=True, capture_output=True,
+                       text=True)
+        fin, fout = os.path.join(td, "in.u16"), os.path.join(td, "out.c64")
+        x.tofile(fin)
+        r = subprocess.run([exe, str(fftpoint), fin, fout], capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, (r.returncode, r.stderr)
+        y = np.fromfile(fout, np.complex64).reshape(calls, 4 * blk)
+    conc = np.concatenate([y[c, :3 * blk].reshape(3, blk) for c in range(calls)], 1)
+    single = np.concatenate([y[c, 3 * blk:] for c in range(calls)])
+    dms = [0.5, 20.0, 60.0]
+    d = Dedisperser(16e6, dms, 1242e6, fftpoint, count, precision="fp16")
+    o = O.Dedisp(16e6, dms, 1242e6, fftpoint, count)
+    py, ref = [], []
+    for c in range(calls):
+        blk_in = x[c * blk:(c + 1) * blk]
+        d.filter_block(blk_in)
+        py.append(d.get_output())
+        ref.append(o.filter(O.decode_uint16(blk_in)))
+    py, ref = np.concatenate(py, 1), np.concatenate(ref, 1)
+    np.testing.assert_array_equal(conc, py)
+    np.testing.assert_array_equal(single, py[1])
+    for i in range(3):
+        e = float(np.sqrt(np.mean(np.abs(conc[i] - ref[i]) ** 2) / np.mean(np.abs(ref[i]) ** 2)))
+        assert e < 1.5e-3, (dms[i], e)
+
+
+@pytest.mark.gpu
 def test_fold_raw_state_and_per_trial_prepare_fields():
     import oracle as O
     src = os.path.join(ROOT, "tests", "cpp", "fold_state_demo.cpp")
