@@ -86,3 +86,35 @@ def test_batch_rejects_a_handle_twice():
     d = make(OBS[0])
     with pytest.raises(_abi.MsosmError):
         DedispBatch([d, d])
+
+
+def test_batch_groups_by_precision_and_size():
+    # bf16 members at FFT 8192 and 16384 and an f16 member at 16384 form three
+    # kernel groups; each member's profiles equal its own handle's to
+    # rounding, and its series is within the bf16 / f16 bound of the oracle
+    obs = [(16e6, 1242e6, [1.0, 6.0], 8192, 6, "bf16", 0.0011),
+           (16e6, 1242e6, [2.0, 5.0], 16384, 3, "bf16", 0.0011),
+           (16e6, 1242e6, [0.5, 4.0], 16384, 3, "fp16", 0.0011)]
+    batch_h = [make(o) for o in obs]
+    solo_h = [make(o) for o in obs]
+    b = DedispBatch(batch_h)
+    assert b.info()["groups"] == 3
+    orc = [O.Dedisp(o[0], o[2], o[1], o[3], o[4]) for o in obs]
+    rng = np.random.default_rng(9)
+    for c in range(4):
+        xs = [((rng.standard_normal(d.block_samples) + 1j * rng.standard_normal(d.block_samples)) * 300)
+              .astype(np.complex64) for d in batch_h]
+        b.filter_block(xs)
+        for d, s, o, x, ob in zip(batch_h, solo_h, orc, xs, obs):
+            s.filter_block(x)
+            ref = o.filter(x.astype(np.complex128))
+            y, ys = d.get_output(), s.get_output()
+            for t in range(d.numDMs):
+                assert rel_rms(y[t], ys[t]) < 1e-6
+                assert rel_rms(y[t], ref[t]) < (1e-2 if ob[5] == "bf16" else SERIES_TOL)
+    for d, s in zip(batch_h, solo_h):
+        assert d.folded_periods() == s.folded_periods() > 0
+        p, ps = d.get_profiles().astype(np.float64), s.get_profiles().astype(np.float64)
+        for t in range(d.numDMs):
+            assert rel_rms(p[t], ps[t]) < 1e-6
+    b.close()
