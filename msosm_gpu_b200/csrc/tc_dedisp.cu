@@ -266,12 +266,27 @@ __device__ __forceinline__ float warp_max(float v)
 //   GEMM 2, B2[n][k1], k1 < 64: n < 32 -> cos(2 pi k1 (32 + n) / 64),
 //     n >= 32 -> sin(2 pi k1 n / 64)                   (output m1 = 32..63)
 // At N = 16384 (N1 = N2 = 128) GEMM 2 reads B1's columns 64..127 (C) and
-// 192..255 (S) instead of a B2.
+// 192..255 (S) instead of a B2.  At N = 4096 (N1 = N2 = 64) the paired
+// tables of TcShape::PAIRED replace B1 and B2 (filled by the first branch).
 template <class E, int LOG2N>
 __device__ void fill_constants(unsigned char *sm, int tid)
 {
     using S = TcShape<LOG2N>;
     constexpr int N2 = S::N2;
+    if constexpr (S::PAIRED) {
+        // column n: quarter q = n / 32 holds C (q even) or S (q odd) of
+        // frequency m = n % 32 (q < 2) or 32 + n % 32 (q >= 2); B1N holds -S
+        // where B1 holds C, and C where it holds S
+        for (int e = tid; e < 2 * N2 * N2; e += (int)blockDim.x) {
+            const int n = e / N2, k = e % N2, q = n >> 5, m = (n & 31) + (q >= 2 ? 32 : 0);
+            float s, c;
+            sincospif((float)((k * m) & (N2 - 1)) * (2.0f / N2), &s, &c);
+            const int off = k_off(n, k, (int)S::SBO_B1);
+            *reinterpret_cast<typename E::h1 *>(sm + S::SMEM_B1 + off) = E::one((q & 1) ? s : c);
+            *reinterpret_cast<typename E::h1 *>(sm + S::SMEM_B1N + off) = E::one((q & 1) ? c : -s);
+        }
+        return;
+    }
     for (int e = tid; e < 2 * N2 * N2; e += (int)blockDim.x) {
         const int n = e / N2, k = e % N2;
         float s, c;
@@ -366,11 +381,31 @@ __device__ __forceinline__ void issue_cgemm_cs(uint32_t tmem_d, uint32_t a, uint
 }
 
 // GEMM 1 of a step (operand buffer at a), committed to bar
+// Re x T + Im x T' into n columns at tmem_d: the data (K = 2 x ksteps of
+// 16, Re then Im, MN-major at a) against the paired tables T at b and T' at
+// bn (N = n, K-major, N-group stride sbo).  Half the MMAs of issue_cgemm's
+// three passes, each of full width.
+template <class E>
+__device__ __forceinline__ void issue_paired(uint32_t tmem_d, uint32_t a, uint32_t b, uint32_t bn, int n, int ksteps,
+                                             uint32_t sbo)
+{
+    const uint32_t id = idesc_f16(128, n, true, false, E::fmt);
+    const uint64_t da = smem_desc(a, 2048, 128), db = smem_desc(b, 128, sbo), dn = smem_desc(bn, 128, sbo);
+    const uint64_t sa = kDescStepA >> 4, sb = kDescStepB >> 4;
+    for (int s = 0; s < ksteps; ++s)
+        mma_f16(tmem_d, da + s * sa, db + s * sb, id, s > 0 ? 1u : 0u);
+    for (int s = 0; s < ksteps; ++s)
+        mma_f16(tmem_d, da + (ksteps + s) * sa, dn + s * sb, id, 1u);
+}
+
 template <class E, int LOG2N>
 __device__ __forceinline__ void issue_gemm1(uint32_t tmem, uint32_t s0, uint32_t a, uint32_t bar)
 {
     using S = TcShape<LOG2N>;
-    issue_cgemm<E>(tmem, a, s0 + S::SMEM_B1, S::N2, S::N2 / 16, S::SBO_B1);
+    if constexpr (S::PAIRED)
+        issue_paired<E>(tmem, a, s0 + S::SMEM_B1, s0 + S::SMEM_B1N, 2 * S::N2, S::N2 / 16, S::SBO_B1);
+    else
+        issue_cgemm<E>(tmem, a, s0 + S::SMEM_B1, S::N2, S::N2 / 16, S::SBO_B1);
     mma_commit(bar);
 }
 
@@ -385,6 +420,13 @@ __device__ __forceinline__ void issue_gemm2(uint32_t tmem, uint32_t s0, uint32_t
     if constexpr (S::N1 == 128) {
         issue_cgemm_cs<E>(tmem + S::D2_COL, a, s0 + S::SMEM_B1 + 8 * S::SBO_B1, s0 + S::SMEM_B1 + 24 * S::SBO_B1,
                           S::D2_HALF, S::N1 / 16, S::SBO_B1);
+    } else if constexpr (S::PAIRED) {
+        // [C_hi | S_hi] and [-S_hi | C_hi]: the tables' columns 64..127.  The
+        // three-pass forms of both GEMMs issued 24 MMAs per pair instead of
+        // 16; thread 0's issue is on the CTA's critical path, and the kernel
+        // ran 4 % slower (19.05 vs 18.63 ms per 2^24 samples x 256 trials)
+        issue_paired<E>(tmem + S::D2_COL, a, s0 + S::SMEM_B1 + 8 * S::SBO_B1, s0 + S::SMEM_B1N + 8 * S::SBO_B1, 64, 4,
+                        S::SBO_B1);
     } else {
         issue_cgemm<E>(tmem + S::D2_COL, a, s0 + S::SMEM_B2, 32, 4, 1024);
         if constexpr (S::N2 == 128)
@@ -756,11 +798,14 @@ __global__ void __launch_bounds__(TcShape<LOG2N>::THREADS, TcShape<LOG2N>::CTAS_
             for (int p = 0; p < 2; ++p) {
                 float re[16], im[16];
                 uint32_t w8r[8], w8i[8];
+                // D1 columns of m2 = 32 g + 16 p + 0..15: Re and Im N2 apart,
+                // or with the paired tables 32 apart within quarters 2 g, 2 g + 1
+                const uint32_t cre = S::PAIRED ? 64 * g + 16 * p : 32 * g + 16 * p;
+                const uint32_t cim = S::PAIRED ? 64 * g + 32 + 16 * p : N2 + 32 * g + 16 * p;
                 if constexpr (kTwInTmem)
-                    tmem_ld_twiddle(tD1 + 32 * g + 16 * p, tD1 + N2 + 32 * g + 16 * p, tTW + 8 * p, tTW + 16 + 8 * p,
-                                    re, im, w8r, w8i);
+                    tmem_ld_twiddle(tD1 + cre, tD1 + cim, tTW + 8 * p, tTW + 16 + 8 * p, re, im, w8r, w8i);
                 else
-                    tmem_ld_2x16(tD1 + 32 * g + 16 * p, tD1 + N2 + 32 * g + 16 * p, re, im);
+                    tmem_ld_2x16(tD1 + cre, tD1 + cim, re, im);
                 uint32_t pr[8], pim[8];
 #pragma unroll
                 for (int i = 0; i < 8; ++i) {
@@ -957,15 +1002,10 @@ __global__ void __launch_bounds__(kThreads, 1) tc_probe_kernel(int step, const u
     const uint32_t tcol = step == 1 ? 0u : (uint32_t)S::D2_COL;
     if (tid == 0) {
         tc_fence_after();
-        if (step == 1) {
-            issue_cgemm<F16>(tmem, s0 + S::SMEM_OP0, s0 + S::SMEM_B1, S::N2, S::N2 / 16, S::SBO_B1);
-            mma_commit(bar);
-        } else if constexpr (S::N1 == 128) {
+        if (step == 1)
+            issue_gemm1<F16, LOG2N>(tmem, s0, s0 + S::SMEM_OP0, bar);
+        else
             issue_gemm2<F16, LOG2N>(tmem, s0, s0 + S::SMEM_OP0, bar);
-        } else {
-            issue_cgemm<F16>(tmem + tcol, s0 + S::SMEM_OP0, s0 + S::SMEM_B2, 32, 4, 1024);
-            mma_commit(bar);
-        }
     }
     uint32_t parity = 0;
     if (!wait_gemm(tid, bar, parity)) {
@@ -979,12 +1019,19 @@ __global__ void __launch_bounds__(kThreads, 1) tc_probe_kernel(int step, const u
     const int ncol = step == 1 ? 2 * S::N2 : 2 * S::D2_HALF;
     const int row = 32 * (warp & 3) + lane, h = warp >> 2;
     const uint32_t base = tmem + tcol + ((uint32_t)(32 * (warp & 3)) << 16);
+    // D column of TMEM column c: [Re | Im] of the output frequency; the paired
+    // GEMM 1 leaves [Re_lo | Im_lo | Re_hi | Im_hi] (32 frequencies each)
+    auto dcol = [&](int c) {
+        if (!(S::PAIRED && step == 1))
+            return c;
+        return (((c >> 5) & 1) ? 64 : 0) + ((c >> 6) ? 32 : 0) + (c & 31);
+    };
     for (int c0 = h * ncol / 2; c0 < (h + 1) * ncol / 2; c0 += 32) {
         float x[16], y[16];
         tmem_ld_2x16(base + c0, base + c0 + 16, x, y);
         for (int i = 0; i < 16; ++i) {
-            D[row * ncol + c0 + i] = x[i];
-            D[row * ncol + c0 + 16 + i] = y[i];
+            D[row * ncol + dcol(c0 + i)] = x[i];
+            D[row * ncol + dcol(c0 + 16 + i)] = y[i];
         }
     }
     tc_teardown<LOG2N>(tmem, warp);

@@ -49,11 +49,20 @@ struct TcShape {
     static constexpr int THREADS = 32 * WARPS;         // 256 or 512
     static constexpr int CTAS_PER_SM = LOG2N == 12 ? 2 : 1;
     static constexpr int B1_BYTES = 2 * N2 * N2 * 2;                  // [C | S]: 2 N2 columns x N2 K, 16-bit
-    static constexpr int B2_BYTES = LOG2N == 14 ? 0 : 64 * 64 * 2;    // [C | S]: 64 columns x 64 K
+    // At N = 4096 (N1 = N2 = 64) both GEMMs are 64-point DFTs: B1 holds
+    // [C_lo | S_lo | C_hi | S_hi] (32 frequencies each, lo = 0..31, hi =
+    // 32..63) and B1N the companion [-S_lo | C_lo | -S_hi | C_hi], so each
+    // GEMM is Re x B1 + Im x B1N (GEMM 2 on columns 64..127): 8 MMAs each
+    // instead of 12, no B2 table, the same shared memory.  GEMM 1 then
+    // leaves D1 as [Re_lo | Im_lo | Re_hi | Im_hi].
+    static constexpr bool PAIRED = LOG2N == 12;
+    static constexpr int B2_BYTES = LOG2N == 13 ? 64 * 64 * 2 : 0;    // [C | S]: 64 columns x 64 K
+    static constexpr int B1N_BYTES = PAIRED ? 2 * N2 * N2 * 2 : 0;
     static constexpr int OP_BYTES = 128 * 2 * N2 * 2;    // GEMM 1 data operand (128 rows x 2 N2 K)
     static constexpr int SMEM_B1 = 0;
     static constexpr int SMEM_B2 = B1_BYTES;
-    static constexpr int SMEM_OP0 = B1_BYTES + B2_BYTES;  // two operand buffers; a buffer then
+    static constexpr int SMEM_B1N = B1_BYTES + B2_BYTES;
+    static constexpr int SMEM_OP0 = B1_BYTES + B2_BYTES + B1N_BYTES;  // two operand buffers; a buffer then
     static constexpr int SMEM_OP1 = SMEM_OP0 + OP_BYTES;  // holds its step's intensities
     static constexpr int SMEM_CTL = SMEM_OP1 + OP_BYTES;  // mbarriers, TMEM address, per-warp maxima
     static constexpr int SMEM_FOLD = SMEM_CTL + 256;      // fold span window, partials, profiles
@@ -68,17 +77,8 @@ struct TcShape {
 };
 
 constexpr int kLog2NMin = 12, kLog2NMax = 14;
-// the 4096-point shape (also the GEMM layout check's)
-constexpr int kLog2N = 12;
-constexpr int kN = 1 << kLog2N, kM = kN / 2;
+// threads of the GEMM layout check (tc_probe_kernel)
 constexpr int kThreads = 256;
-constexpr int kSmemB1 = TcShape<12>::SMEM_B1;
-constexpr int kSmemB2 = TcShape<12>::SMEM_B2;
-constexpr int kSmemOp0 = TcShape<12>::SMEM_OP0;
-constexpr int kSmemOp1 = TcShape<12>::SMEM_OP1;
-constexpr int kSmemCtl = TcShape<12>::SMEM_CTL;
-constexpr int kSmemFold = TcShape<12>::SMEM_FOLD;
-constexpr int kTmemCols = 256;
 
 // MN-major data operand (K groups 2048 B apart, row groups 128 B): element
 // (row r, k) -> byte offset
