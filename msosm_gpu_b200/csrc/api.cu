@@ -235,10 +235,20 @@ msosm_status design_filters(int log2n, const std::vector<ChirpParams> &cp, float
     return MSOSM_OK;
 }
 
-// Profiles of up to this many bins live in shared memory inside the fused
-// kernel (beyond it, in the global partial rows): the 8192- and 16384-point
-// tensor-core kernels leave room for 2048.
-int smem_bins_limit(const msosm_dedisp *d) { return d->tc && d->log2n >= 13 ? 2048 : kMaxSmemBins; }
+// Whether the fused kernel keeps a work item's two profiles in shared memory
+// (else in the global partial rows): up to kMaxSmemBins bins, and in the
+// tensor-core kernels only when they fit beside the tables, operand buffers
+// and span window in the device's per-block limit (at 8192 points that is
+// 1024 bins with the usual 64-span window; at 16384, 2048).
+bool prof_in_smem(const msosm_dedisp *d)
+{
+    if (d->nbins > kMaxSmemBins)
+        return false;
+    if (!d->tc)
+        return true;
+    const size_t need = tc_smem_base(d->log2n) + fold_smem_bytes(d->nbins, d->win_cap, true, tc_threads(d->log2n));
+    return need <= tc_smem_limit();
+}
 
 // Persistent grid of the dedispersion kernel: work items (block range,
 // trial), about eight per resident CTA, spread evenly over the waves.
@@ -251,7 +261,7 @@ cudaError_t plan_grid(msosm_dedisp *d)
     if (e != cudaSuccess)
         return e;
     const int threads = d->tc ? tc_threads(d->log2n) : (int)(d->N / 16);
-    const size_t extra = d->fold ? fold_smem_bytes(d->nbins, d->win_cap, d->nbins <= smem_bins_limit(d), threads) : 0;
+    const size_t extra = d->fold ? fold_smem_bytes(d->nbins, d->win_cap, prof_in_smem(d), threads) : 0;
     int per_sm = d->tc ? tc_blocks_per_sm(d->log2n, d->tc_bf16, d->series, d->fold, extra)
                        : dedisp_blocks_per_sm(d->log2n, d->pingpong, d->series, d->fold, extra);
     if (per_sm < 1)
@@ -897,7 +907,7 @@ static msosm_status fold_prepare(msosm_dedisp *d, int sb, FoldArgs &fa)
     fa.detect = d->detect;
     fa.part_main = d->part_main;
     fa.part_pend = d->part_pend;
-    fa.smem_prof = d->nbins <= smem_bins_limit(d) ? 1 : 0;
+    fa.smem_prof = prof_in_smem(d) ? 1 : 0;
     fa.span_cap = d->win_cap;
     fa.inv_bpt = 1.0f / (float)d->bpt;
     fa.g_shift = fold_g_shift(d->bpt, d->large ? 256 : (int)(d->N / 16));
@@ -1234,7 +1244,7 @@ msosm_status msosm_batch_create(msosm_dedisp *const *handles, int n, msosm_batch
         for (int i : g.members) {
             const msosm_dedisp *d = b->h[i];
             if (g.fold)
-                g.fold_smem = std::max(g.fold_smem, fold_smem_bytes(d->nbins, d->win_cap, d->nbins <= smem_bins_limit(d),
+                g.fold_smem = std::max(g.fold_smem, fold_smem_bytes(d->nbins, d->win_cap, prof_in_smem(d),
                                                                     tc_threads(d->log2n)));
         }
         int per_sm = tc_blocks_per_sm(g.log2n, g.bf16, g.series, g.fold, g.fold_smem);

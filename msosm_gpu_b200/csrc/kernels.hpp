@@ -147,6 +147,11 @@ bool tc_supported(int log2n);
 int tc_threads(int log2n);
 // blocks one step of the kernel transforms: 2 (a pair) at 4096 and 8192, 1 at 16384
 int tc_blocks_per_step(int log2n);
+// shared memory of the tensor-core kernel before its fold state (tables,
+// operand buffers, control), and the device's per-block limit (0 when it
+// cannot be read)
+size_t tc_smem_base(int log2n);
+size_t tc_smem_limit();
 int tc_blocks_per_sm(int log2n, bool bf16, bool series, bool fold, size_t extra_smem);
 // a.H and a.delays in tensor-core order (tc_layout.hpp), ring written with
 // FwdArgs::tc_order; a.R counts ranges of steps (tc_blocks_per_step blocks

@@ -58,11 +58,15 @@ struct TcShape {
     static constexpr bool PAIRED = LOG2N == 12;
     static constexpr int B2_BYTES = LOG2N == 13 ? 64 * 64 * 2 : 0;    // [C | S]: 64 columns x 64 K
     static constexpr int B1N_BYTES = PAIRED ? 2 * N2 * N2 * 2 : 0;
+    // at N = 8192 (GEMM 1 128-point, GEMM 2 64-point) [-S | C] beside B2, so
+    // that each block's GEMM 2 is Re x B2 + Im x B2N: 8 MMAs instead of 12
+    static constexpr int B2N_BYTES = LOG2N == 13 ? 64 * 64 * 2 : 0;
     static constexpr int OP_BYTES = 128 * 2 * N2 * 2;    // GEMM 1 data operand (128 rows x 2 N2 K)
     static constexpr int SMEM_B1 = 0;
     static constexpr int SMEM_B2 = B1_BYTES;
     static constexpr int SMEM_B1N = B1_BYTES + B2_BYTES;
-    static constexpr int SMEM_OP0 = B1_BYTES + B2_BYTES + B1N_BYTES;  // two operand buffers; a buffer then
+    static constexpr int SMEM_B2N = B1_BYTES + B2_BYTES + B1N_BYTES;
+    static constexpr int SMEM_OP0 = B1_BYTES + B2_BYTES + B1N_BYTES + B2N_BYTES;  // two operand buffers; a buffer then
     static constexpr int SMEM_OP1 = SMEM_OP0 + OP_BYTES;  // holds its step's intensities
     static constexpr int SMEM_CTL = SMEM_OP1 + OP_BYTES;  // mbarriers, TMEM address, per-warp maxima
     static constexpr int SMEM_FOLD = SMEM_CTL + 256;      // fold span window, partials, profiles
