@@ -1134,10 +1134,11 @@ def run_single_dm(args):
              "msosm_fp16": dict(fftpoint=c["fftpoint"], osm=False, precision="fp16"),
              "osm_fp32": dict(fftpoint=c["osm_fftpoint"], osm=True, precision="fp32")}
 
-    def handle(kw, count, series):
+    def handle(kw, count, series, fold=True):
         d = Dedisperser(bw, [p["dm"]], f0, kw["fftpoint"], count=count, osm=kw["osm"], series=series,
                         precision=kw["precision"])
-        d.fold_init(p["period"], bw, time_bin=nb, discard_Nd=nd, detect="power")
+        if fold:
+            d.fold_init(p["period"], bw, time_bin=nb, discard_Nd=nd, detect="power")
         return d
 
     out = {}
@@ -1174,6 +1175,9 @@ def run_single_dm(args):
         # every call's series copied back to pinned host memory
         de = handle(kw, call // M, False)
         ds = handle(kw, call // M, True)
+        # the timed series arm does what the reference's drivers do per call
+        # (filter, copy the series back) and no fold
+        dsn = handle(kw, call // M, True, fold=False)
         ser = np.empty(call + 1, np.complex64)
         ser = torch.from_numpy(ser.view(np.float32)).pin_memory().numpy().view(np.complex64)
         keep = []
@@ -1184,12 +1188,12 @@ def run_single_dm(args):
             return de.get_profiles()
 
         def e2e_series(collect=False):
+            h = ds if collect else dsn
             for i in range(ncalls):
-                ds.filter_block(uh[i * call:(i + 1) * call])
-                ds.get_output(out=ser)
+                h.filter_block(uh[i * call:(i + 1) * call])
+                h.get_output(out=ser)
                 if collect:
                     keep.append(ser[:-1].copy())
-            return ds.get_profiles()
 
         e2e_series(collect=True)
         series_of[name] = (np.concatenate(keep), ds.get_profiles()[0].copy())
@@ -1205,6 +1209,7 @@ def run_single_dm(args):
             res[key] = (time.perf_counter() - t0) / args.steps
         de.close()
         ds.close()
+        dsn.close()
         out[name] = {
             "value": samples / (ms * 1e-3) / 1e6, "ms_per_step": ms, "unit": "Msamples/s (1 DM trial)",
             "fftpoint": kw["fftpoint"], "precision": kw["precision"], "clocks": ck.summary(),
